@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""X-engine benchmark: libxgpu.so on B200 vs the reference's CPU engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU; with --gpus N every rank runs it on its own channels, so
+per-GPU work is fixed: weak scaling, no collective): xGPU's default build
+shape, NSTATION=256, NPOL=2, NFREQUENCY=10, NTIME=1024, Gaussian int8 samples
+(sigma 16, seeded).  A step is one xgpuCudaXengine call's worth of samples
+correlated by the tcgen05 int8 engine into the int64 integration buffer.
+
+* value      -- X-engine TOPS (16*F*T*N(N+1) ops per step, the flop count of
+                xGPU kernel.cuh:419) with the input resident in HBM, K steps
+                timed with CUDA events on the engine's stream, the input
+                rotating over buffers larger than L2 in total.
+* e2e        -- the same metric through the reference-facing call sequence
+                with host buffers: xgpuClearDeviceIntegrationBuffer +
+                xgpuCudaXengine(SYNCOP_DUMP), i.e. pinned host -> device copy,
+                correlation, device-side formatting and the device -> host
+                dump inside every step (one integration of one dump).
+* detail     -- the plain CUDA-core dp4a and FP32 engines on the same
+                workload, and the tensor engine at NSTATION=512, NFREQUENCY=256,
+                NTIME=8192 (one block of the large-array configuration).
+* cpu_baseline / --impl reference -- the reference's own xgpuOmpXengine
+                (src/omp_xengine.c built with -fopenmp under oracle/_ref, DP4A
+                variant) on all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "X-engine TOPS: int8-TC vs plain @N=256/512, bit-exact; served p50/p99 dump ms"
+N, F, T = 256, 10, 1024
+N3, F3, T3 = 512, 256, 8192
+SIGMA = 16.0
+L2_BYTES = 126 * 1024 * 1024
+
+
+def ops(n, f, t):
+    return 16.0 * f * t * n * (n + 1)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "MEASURED_PEAKS.json"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback (no MEASURED_PEAKS.json)"
+
+
+def read_profile_traffic():
+    """Per-launch DRAM bytes of the tensor kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "xengine_tc_kernel_n256.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a run."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.fh.seek(0)
+        rows = [r.split(",") for r in self.fh.read().splitlines() if r.strip()]
+        os.unlink(self.fh.name)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                clk, mx, pw = float(r[1]), float(r[2]), float(r[3])
+            except (ValueError, IndexError):
+                continue
+            smax = max(smax, mx)
+            if pw > 200.0:  # under load
+                sm.append(clk)
+            for nm, v in zip(names, r[5:9]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(nm)
+        if not sm:
+            sm = [float(r[1]) for r in rows if len(r) > 1 and r[1].strip().replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, seed=1,
+                     sigma=SIGMA, min_rotate_bytes=2 * L2_BYTES, max_bufs=16):
+    """Average ms per xgpuCudaXengineDevice call (input resident in HBM)."""
+    c = xg.Correlator(n, f, t, engine=engine, compute=compute, output="int32", order="tri",
+                      device=torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    c.set_stream(stream.cuda_stream)
+    nbytes = int(c.info.vecLength) * 2
+    nbuf = max(1, min(max_bufs, -(-min_rotate_bytes // nbytes)))
+    bufs = []
+    for q in range(nbuf):
+        b = torch.empty(nbytes, dtype=torch.int8, device="cuda")
+        xg.generate_device(b.data_ptr(), nbytes, 0, seed + q, sigma, torch.cuda.current_device())
+        bufs.append(b)
+    for k in range(warmup):
+        c.run_device(bufs[k % nbuf].data_ptr(), xg.SYNCOP_NONE)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        c.run_device(bufs[k % nbuf].data_ptr(), xg.SYNCOP_NONE)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1) / steps
+    c.close()
+    del bufs
+    torch.cuda.empty_cache()
+    return ms, nbuf * nbytes
+
+
+def e2e_ms(xg, oracle, n, f, t, steps, warmup, device):
+    """Wall ms per integration through xgpuCudaXengine with pinned host buffers."""
+    c = xg.Correlator(n, f, t, engine="tensor", output="int32", order="tri", device=device)
+    x = oracle.gaussian_input(n, f, t, seed=1, sigma=SIGMA)
+    c.set_input(x)
+    for _ in range(warmup):
+        c.clear()
+        c.run(xg.SYNCOP_DUMP)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        c.clear()
+        c.run(xg.SYNCOP_DUMP)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    h2d = int(c.info.vecLength) * 2
+    d2h = int(c.info.matLength) * 8
+    # the last dump must equal the oracle
+    got = c.output_view()[: c.info.matLength * 2]
+    ok = bool((got == oracle.xengine_i64(x, n, f, t).astype("int32")).all())
+    c.close()
+    return ms, h2d, d2h, ok
+
+
+def int8_peak_tops(torch):
+    """Dense int8 tensor throughput of cuBLASLt (torch._int_mm) at 8192^3."""
+    try:
+        m = 8192
+        a = torch.randint(-128, 127, (m, m), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (m, m), dtype=torch.int8, device="cuda").t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 5)
+        return 2.0 * m ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
+def cpu_baseline(steps_cap=None, budget_s=12.0):
+    """The reference's xgpuOmpXengine on the host, DP4A build, this workload."""
+    import oracle
+    if not oracle.ref_available("c2", "dp4a_rt"):
+        return None
+    R = oracle.RefLib("c2", "dp4a_rt")
+    x = oracle.gaussian_input(N, F, T, seed=1, sigma=SIGMA)
+    R.omp_xengine(x)  # warm
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        R.omp_xengine(x)
+        times.append(time.perf_counter() - t0)
+        if steps_cap and len(times) >= steps_cap:
+            break
+        if time.perf_counter() - t_start > budget_s and len(times) >= 3:
+            break
+    med = statistics.median(times)
+    return {"value": ops(N, F, T) / med / 1e12, "unit": "TOPS", "cores": os.cpu_count(),
+            "kind": "reference",
+            "sample": f"{len(times)} full calls of xgpuOmpXengine (src/omp_xengine.c, -O3 -fopenmp, "
+                      f"DP4A build) at N={N} F={F} T={T}; median {med * 1e3:.1f} ms per call",
+            "ms_per_call": med * 1e3}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    base = {"metric": METRIC, "unit": "TOPS", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True}
+    if not oracle.ref_available("c2", "dp4a_rt"):
+        base["unavailable"] = "reference CPU engine not built (oracle/_ref missing)"
+        print(json.dumps(base))
+        return
+    R = oracle.RefLib("c2", "dp4a_rt")
+    x = oracle.gaussian_input(N, F, T, seed=1, sigma=SIGMA)
+    for _ in range(args.warmup):
+        R.omp_xengine(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        R.omp_xengine(x)
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    v = ops(N, F, T) / (ms * 1e-3) / 1e12
+    base.update({
+        "value": v, "ms_per_step": ms, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+        "data": "synthetic: seeded Gaussian int8, sigma 16",
+        "config": {"workload": f"xgpuOmpXengine NSTATION={N} NPOL=2 NFREQUENCY={F} NTIME={T}, "
+                               "one call per step", "nstation": N, "nfrequency": F, "ntime": T},
+        "cpu_baseline": {"value": v, "unit": "TOPS", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"{args.steps} calls of the reference xgpuOmpXengine (DP4A "
+                                   "build, OpenMP on all host cores)"},
+        "e2e": {"value": v, "unit": "TOPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+    print(json.dumps(base))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-detail", action="store_true", help="skip the plain/N=512 legs")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    import oracle
+    import xgpu_b200 as xg
+    torch.cuda.set_device(local)
+    clocks = Clocks(local)
+
+    # headline: tensor engine, config 2, input resident in HBM
+    ms, rot_bytes = device_engine_ms(xg, torch, "tensor", "int8", N, F, T, args.steps,
+                                     args.warmup, world)
+    ms = max_over_ranks(world, ms)
+    value = world * ops(N, F, T) / (ms * 1e-3) / 1e12
+
+    detail = {}
+    if not args.no_detail:
+        k2 = max(3, min(args.steps, 50))
+        ms_p, _ = device_engine_ms(xg, torch, "plain", "int8", N, F, T, k2, 3, world)
+        ms_f, _ = device_engine_ms(xg, torch, "plain", "fp32", N, F, T, k2, 3, world)
+        detail["plain_dp4a_n256_tops"] = ops(N, F, T) / (ms_p * 1e-3) / 1e12
+        detail["plain_fp32_n256_tops"] = ops(N, F, T) / (ms_f * 1e-3) / 1e12
+        detail["tc_over_plain_dp4a_n256"] = value / world / detail["plain_dp4a_n256_tops"]
+        k3 = max(3, min(args.steps, 10))
+        ms3, _ = device_engine_ms(xg, torch, "tensor", "int8", N3, F3, T3, k3, 2, world,
+                                  sigma=40.0, min_rotate_bytes=0, max_bufs=1)
+        detail["tc_n512_tops"] = ops(N3, F3, T3) / (ms3 * 1e-3) / 1e12
+        detail["tc_n512_ms_per_block"] = ms3
+
+    e2e_v = None
+    if rank == 0:
+        k_e = max(3, min(args.steps, 50))
+        ms_e, h2d, d2h, ok = e2e_ms(xg, oracle, N, F, T, k_e, 3, local)
+        e2e_v = {"value": ops(N, F, T) / (ms_e * 1e-3) / 1e12, "unit": "TOPS",
+                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e,
+                 "steps": k_e, "bit_exact_vs_oracle": ok}
+    clk = clocks.stop()
+    peak8 = int8_peak_tops(torch) if rank == 0 else None
+    if rank != 0:
+        barrier(world)
+        return
+
+    peaks, peak_src = load_peaks()
+    # Roofline of the tensor kernel at this workload.  Algorithmic bytes per
+    # launch: input 4*F*T*N + int64 integration buffer read and written
+    # (2 * 16 * F * N(N+1)/2 * 4 ... = 2 * F * N(N+1)/2 * 4 pol * 2 * 8 B).
+    in_bytes = 4.0 * F * T * N
+    state_bytes = F * N * (N + 1) / 2 * 4 * 2 * 8
+    alg_bytes = in_bytes + 2 * state_bytes
+    t_s = ms * 1e-3
+    hbm_ach = alg_bytes / t_s / 1e9
+    tops_ach = ops(N, F, T) / t_s / 1e12
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    t_hbm = alg_bytes / (hbm_peak * 1e9)
+    t_tc = ops(N, F, T) / ((peak8 or 2 * float(peaks.get("bf16_tflops", 1590.0))) * 1e12)
+    traffic = read_profile_traffic()
+    if t_hbm >= t_tc:
+        roof = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": hbm_ach / hbm_peak, "traffic": traffic,
+                "peak_source": f"hbm_gbs of {peak_src} (of measured)",
+                "algorithmic_bytes_per_launch": alg_bytes}
+    else:
+        roof = {"bound": "tensor", "achieved": tops_ach, "peak": peak8, "unit": "TOPS",
+                "frac": tops_ach / peak8, "traffic": traffic,
+                "peak_source": "dense int8 cuBLASLt GEMM 8192^3 measured in this run (of measured)"}
+    detail["int8_tensor_peak_tops_measured"] = peak8
+    detail["tc_n256_frac_of_int8_peak"] = tops_ach / peak8 if peak8 else None
+    detail["tc_n256_hbm_gbs"] = hbm_ach
+    if "tc_n512_tops" in detail and peak8:
+        detail["tc_n512_frac_of_int8_peak"] = detail["tc_n512_tops"] / peak8
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "TOPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8",
+        "data": "synthetic: seeded Gaussian int8 samples, sigma 16 (counter-based generator)",
+        "config": {"workload": f"xGPU default shape NSTATION={N} NPOL=2 NFREQUENCY={F} NTIME={T}: "
+                               "one xgpuCudaXengine call per step, tcgen05 int8 engine, int64 "
+                               "integration buffer",
+                   "nstation": N, "npol": 2, "nfrequency": F, "ntime": T,
+                   "parallelism": f"channel-sharded replicas x{world} (no collective)",
+                   "l2": f"input rotates over {rot_bytes / 2**20:.0f} MiB of buffers (> 126 MiB L2)"},
+        "e2e": e2e_v, "gpu_launches": args.steps, "roofline": roof,
+        "cpu_baseline": cpu_baseline(), "clocks": clk, "detail": detail,
+    }
+    print(json.dumps(line))
+    barrier(world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,276 @@
+/*
+ * xgpu.h -- C ABI of the B200 X-engine (libxgpu.so).
+ *
+ * This header is the drop-in surface for programs written against xGPU's
+ * src/xgpu.h.  Every type, macro value, struct layout and prototype that
+ * xGPU declares is declared here with the same name, value and layout, so a
+ * program that compiled and linked against xGPU compiles and links against
+ * this library unchanged.  Citations are to the reference's src/ directory.
+ *
+ * Names that xGPU does not have are marked "extension".  They add runtime
+ * sizing (xGPU fixes every size at library build time), a choice of engine
+ * (CUDA-core 2x2 register tile, or tcgen05 int8 tensor cores), exact int64
+ * integration dumps, device-resident input and the packed 4+4-bit input.
+ */
+#ifndef XGPU_H
+#define XGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Input samples are 8-bit fixed point (xgpu.h:10-20 hard-codes FIXED_POINT). */
+#define FIXED_POINT
+
+#ifndef FIXED_POINT
+typedef float ReImInput;
+#else
+typedef signed char ReImInput;
+#endif
+
+/* One complex input sample, real part first (xgpu.h:22-25). */
+typedef struct ComplexInputStruct {
+  ReImInput real;
+  ReImInput imag;
+} ComplexInput;
+
+/* One output visibility (xgpu.h:27-37).  Callers that define DP4A receive
+ * 32-bit integers; everyone else receives 32-bit floats.  Both are 8 bytes,
+ * so buffer sizes do not depend on the choice.  The library writes whichever
+ * the context was created for (XGPUConfig.output_type). */
+#ifndef DP4A
+typedef struct ComplexStruct {
+  float real;
+  float imag;
+} Complex;
+#else
+typedef struct ComplexStruct {
+  int real;
+  int imag;
+} Complex;
+#endif
+
+/* Type codes (xgpu.h:40-42). */
+#define XGPU_INT8    (0)
+#define XGPU_FLOAT32 (1)
+#define XGPU_INT32   (2)
+
+/* Output matrix orders (xgpu.h:45-47). */
+#define TRIANGULAR_ORDER 1000
+#define REAL_IMAG_TRIANGULAR_ORDER 2000
+#define REGISTER_TILE_TRIANGULAR_ORDER 3000
+
+/* xgpuInit flags (xgpu.h:50-54): the low 16 bits select the CUDA device. */
+#define XGPU_DEVICE_MASK          ((1<<16)-1)
+#define XGPU_DONT_REGISTER_ARRAY  (1<<16)
+#define XGPU_DONT_REGISTER_MATRIX (1<<17)
+#define XGPU_DONT_REGISTER        (XGPU_DONT_REGISTER_ARRAY | \
+                                   XGPU_DONT_REGISTER_MATRIX)
+
+/* Sizing report (xgpu.h:61-92).  Field order and types are unchanged, so the
+ * struct is byte-identical to xGPU's. */
+typedef struct XGPUInfoStruct {
+  unsigned int npol;          /* polarisations per station (always 2) */
+  unsigned int nstation;      /* stations */
+  unsigned int nbaseline;     /* nstation*(nstation+1)/2, autos included */
+  unsigned int nfrequency;    /* channels */
+  unsigned int ntime;         /* samples per channel per xgpuCudaXengine call */
+  unsigned int ntimepipe;     /* samples per host-to-device transfer chunk */
+  unsigned int input_type;    /* XGPU_INT8 */
+  unsigned int compute_type;  /* XGPU_INT8 (integer engines) or XGPU_FLOAT32 */
+  long long unsigned int vecLength;      /* ComplexInput elements per call */
+  long long unsigned int vecLengthPipe;  /* ComplexInput elements per chunk */
+  long long unsigned int matLength;      /* Complex elements in the output */
+  long long unsigned int triLength;      /* Complex elements in triangular order */
+  unsigned int matrix_order;  /* one of the *_ORDER codes */
+  size_t shared_atomic_size;  /* kept for layout compatibility; reports 4 */
+  size_t complex_block_size;  /* kept for layout compatibility; reports 1 */
+} XGPUInfo;
+
+/* Caller-owned context (xgpu.h:94-113), byte-identical to xGPU's. */
+typedef struct XGPUContextStruct {
+  ComplexInput *array_h;   /* host input */
+  Complex *matrix_h;       /* host output */
+  size_t array_len;        /* in ComplexInput units */
+  size_t matrix_len;       /* in Complex units */
+  size_t input_offset;     /* reset to 0 by xgpuSetHostInputBuffer */
+  size_t output_offset;    /* reset to 0 by xgpuSetHostOutputBuffer */
+  void *internal;          /* opaque library state */
+} XGPUContext;
+
+/* Return codes (xgpu.h:116-121). */
+#define XGPU_OK                          (0)
+#define XGPU_OUT_OF_MEMORY               (1)
+#define XGPU_CUDA_ERROR                  (2)
+#define XGPU_INSUFFICIENT_TEXTURE_MEMORY (3)
+#define XGPU_NOT_INITIALIZED             (4)
+#define XGPU_HOST_BUFFER_NOT_SET         (5)
+/* Extension: a size, pointer, offset or option was out of range.  No call
+ * that xGPU can make with valid arguments returns it. */
+#define XGPU_INVALID_ARGUMENT            (6)
+
+/* syncOp values for xgpuCudaXengine (xgpu.h:124-127). */
+#define SYNCOP_NONE           0
+#define SYNCOP_DUMP           1
+#define SYNCOP_SYNC_TRANSFER  2
+#define SYNCOP_SYNC_COMPUTE   3
+
+/* ------------------------------------------------------------------------ */
+/* Functions of xGPU's cuda_xengine.cu (xgpu.h:134-219).                    */
+/* ------------------------------------------------------------------------ */
+
+/* Library version string (xgpu.h:134); static storage, do not free. */
+const char * xgpuVersionString();
+
+/* Default sizes of this build (xgpu.h:140): the sizes xgpuInit uses.  Set at
+ * library build time with make NSTATION=... NFREQUENCY=... NTIME=...
+ * NTIME_PIPE=... exactly as xGPU's Makefile takes them. */
+void xgpuInfo(XGPUInfo *pcxs);
+
+/* Create a context on device (device_flags & XGPU_DEVICE_MASK) with the
+ * build's default sizes (xgpu.h:168, cuda_xengine.cu:180-331).  Host buffers
+ * follow xGPU's rules: a NULL array_h / matrix_h is allocated pinned by the
+ * library; a non-NULL one is registered (page-rounded) unless the matching
+ * XGPU_DONT_REGISTER_* flag is set.  Unlike xGPU this never calls exit(): no
+ * device gives XGPU_CUDA_ERROR.  The engine is the tcgen05 tensor-core
+ * engine unless the environment variable XGPU_ENGINE=plain selects the
+ * CUDA-core engine. */
+int xgpuInit(XGPUContext *context, int device_flags);
+
+/* Zero the device integration buffer: the next call starts a new
+ * integration (xgpu.h:174, cuda_xengine.cu:334-348). */
+int xgpuClearDeviceIntegrationBuffer(XGPUContext *context);
+
+/* Replace the host input / output buffer (xgpu.h:188,202;
+ * cuda_xengine.cu:354-498).  The previous buffer is freed or unregistered,
+ * and input_offset / output_offset are reset to 0. */
+int xgpuSetHostInputBuffer(XGPUContext *context);
+int xgpuSetHostOutputBuffer(XGPUContext *context);
+
+/* Release everything the context holds (xgpu.h:204, cuda_xengine.cu:501-541).
+ * Safe to call twice. */
+void xgpuFree(XGPUContext *context);
+
+/* Correlate ntime samples at array_h + input_offset and add them to the
+ * device integration buffer (xgpu.h:206-219, cuda_xengine.cu:543-677).
+ *   SYNCOP_NONE          return once the work is queued
+ *   SYNCOP_DUMP          wait, then write the integration (in the context's
+ *                        matrix order and output type) to
+ *                        matrix_h + output_offset; the buffer is not cleared
+ *   SYNCOP_SYNC_TRANSFER wait until the input has been copied to the device
+ *   SYNCOP_SYNC_COMPUTE  wait until the correlation has finished
+ * The device buffer holds exact int64 sums for the integer engines, so an
+ * integration may span any number of calls without overflow; the int32
+ * output of a dump wraps modulo 2^32 exactly as xGPU's int32 buffer does. */
+int xgpuCudaXengine(XGPUContext *context, int syncOp);
+
+/* Extension (named after the dump entry point of later xGPU releases):
+ * wait for queued work, then write the integration to
+ * matrix_h + output_offset exactly as SYNCOP_DUMP does, without correlating
+ * new samples. */
+int xgpuDumpDeviceIntegrationBuffer(XGPUContext *context);
+
+/* ------------------------------------------------------------------------ */
+/* Functions of xGPU's cpu_util.c and omp_xengine.c (xgpu.h:223-235).       */
+/* They use the build's default sizes (xgpuInfo), like xGPU's.  They run on  */
+/* the host and are never part of the device path.                          */
+/* ------------------------------------------------------------------------ */
+
+/* Gaussian noise, sigma 2.5, rounded, saturated to +-7 and scaled by 16, from
+ * the C library rand() stream (cpu_util.c:13-55). */
+void xgpuRandomComplex(ComplexInput* random_num, long long unsigned int length);
+
+/* In-place conversion of a dumped matrix from the default matrix order to
+ * TRIANGULAR_ORDER (cpu_util.c:57-132). */
+void xgpuReorderMatrix(Complex *matrix);
+
+/* Compare two triangular-order matrices and print a summary
+ * (cpu_util.c:134-232). */
+void xgpuCheckResult(Complex *gpu, Complex *cpu, int verbose, ComplexInput *array_h);
+
+/* [t][f][s][p][c] -> [t/4][f][s][p][c][t%4] input swizzle of xGPU's DP4A
+ * builds (cpu_util.c:235-255). */
+void xgpuSwizzleInput(ComplexInput *out, const ComplexInput *in);
+
+/* Triangular order -> full Hermitian [f][i][j][p1][p2] (cpu_util.c:258-279). */
+void xgpuExtractMatrix(Complex *matrix, Complex *packed);
+
+/* Host X-engine in TRIANGULAR_ORDER (omp_xengine.c:36-93), OpenMP over
+ * (channel, baseline).  It sums in int64, so it is exact where xGPU's float
+ * sums round (above 2^24). */
+void xgpuOmpXengine(Complex *matrix_h, ComplexInput *array_h);
+
+/* ------------------------------------------------------------------------ */
+/* Extensions: runtime sizing and engine choice.                            */
+/* ------------------------------------------------------------------------ */
+
+/* Engines. */
+#define XGPU_ENGINE_DEFAULT 0  /* XGPU_ENGINE_TENSOR for integer compute */
+#define XGPU_ENGINE_PLAIN   1  /* CUDA-core 2x2 register tile: FP32 or dp4a */
+#define XGPU_ENGINE_TENSOR  2  /* tcgen05 int8 tensor cores (compute XGPU_INT8) */
+
+/* Input sample formats. */
+#define XGPU_INPUT_INT8     0  /* [t][f][s][p] {re,im} int8 (xGPU's layout) */
+#define XGPU_INPUT_PACKED4  1  /* [t][f][s][p] one byte: re in the high nibble,
+                                  im in the low nibble, 4-bit two's complement */
+#define XGPU_INPUT_DP4A_SWIZZLED 2 /* xgpuSwizzleInput's [t/4][f][s][p][c][t%4] */
+
+typedef struct XGPUConfigStruct {
+  unsigned int nstation;     /* multiple of 16 */
+  unsigned int nfrequency;   /* >= 1 */
+  unsigned int ntime;        /* samples per call, multiple of ntimepipe */
+  unsigned int ntimepipe;    /* multiple of 16 */
+  unsigned int compute_type; /* XGPU_INT8 (exact) or XGPU_FLOAT32 (plain only) */
+  unsigned int output_type;  /* XGPU_FLOAT32 or XGPU_INT32: Complex member type */
+  unsigned int matrix_order; /* TRIANGULAR_ORDER, REAL_IMAG_... or REGISTER_TILE_... */
+  unsigned int engine;       /* XGPU_ENGINE_* */
+  unsigned int input_format; /* XGPU_INPUT_* */
+} XGPUConfig;
+
+/* Fill cfg with this build's defaults (the sizes xgpuInfo reports). */
+void xgpuDefaultConfig(XGPUConfig *cfg);
+
+/* xgpuInit with explicit sizes and options.  Returns XGPU_INVALID_ARGUMENT
+ * for sizes or options outside the documented ranges. */
+int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg);
+
+/* Sizes of an initialised context, in xgpuInfo's form. */
+int xgpuContextInfo(XGPUContext *context, XGPUInfo *info);
+
+/* xgpuCudaXengine on input that is already in device memory (same layout
+ * and size as array_h would hold; 16-byte aligned).  The caller keeps the
+ * buffer unchanged until the call's work is done (any syncOp but NONE, or a
+ * later synchronising call). */
+int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int syncOp);
+
+/* Exact dump: the integration as int64 in triangular order,
+ * [f][baseline][p1][p2][re,im], triLength*2 values, written to host_out.
+ * Integer engines only. */
+int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_out);
+
+/* Fill a device buffer with seeded synthetic samples, identical to the host
+ * generator the tests use: kind 0 = Gaussian int8 with the given sigma,
+ * rounded and clipped to [-127,127]; kind 1 = uniform integers in [-7,7] packed
+ * 4+4-bit (one byte per complex sample); kind 2 = uniform int8 in [-7,7].
+ * nbytes is the buffer size in bytes. */
+int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long long seed,
+                       double sigma, int device);
+
+/* Run the context's device work (engine launches, dump formatting) on the
+ * caller's CUDA stream (a cudaStream_t) instead of the context's own, e.g. to
+ * order it with other work or to bracket it with the caller's CUDA events.
+ * NULL returns to the context's own stream.  The caller keeps the stream alive
+ * until xgpuFree or the next xgpuSetComputeStream. */
+int xgpuSetComputeStream(XGPUContext *context, void *stream);
+
+/* Name of the engine a context runs ("tensor-tcgen05-int8", "plain-dp4a",
+ * "plain-fp32"). */
+const char * xgpuEngineName(XGPUContext *context);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XGPU_H */

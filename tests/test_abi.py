@@ -1,0 +1,178 @@
+"""The C ABI of libxgpu.so, without a GPU.
+
+* the library loads and exports exactly the functions include/xgpu.h declares;
+* include/xgpu.h is layout- and value-compatible with the reference header
+  (sizes, offsets and macro values recorded from it in tests/golden);
+* the host helpers of the reference API (cpu_util.c / omp_xengine.c
+  counterparts) agree with the reference's outputs and with the oracle;
+* host-side error paths return the documented codes (no device present here,
+  bad arguments, use before init, double free).
+"""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "xgpu.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(xgpu[A-Za-z0-9]+)\s*\(", text)))
+
+
+def test_exports_match_header(xg):
+    declared = header_functions()
+    out = subprocess.run(["nm", "-D", "--defined-only", xg.LIB_PATH], check=True,
+                         capture_output=True, text=True).stdout
+    exported = sorted({line.split()[-1] for line in out.splitlines() if " T " in line})
+    assert exported == declared
+    assert sorted(xg.EXPORTED) == declared
+    for name in declared:
+        assert getattr(xg.lib(), name) is not None
+
+
+@pytest.mark.parametrize("tag,flags", [("plain", []), ("dp4a", ["-DDP4A"])])
+def test_header_layout_matches_reference(golden, tag, flags):
+    meta, _ = golden
+    with tempfile.TemporaryDirectory() as td:
+        exe = os.path.join(td, "probe")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), *flags, "-o", exe,
+                        os.path.join(ROOT, "tests", "golden", "abi_probe.c")], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    ours = {k: int(v) for k, v in (line.split() for line in out.splitlines())}
+    assert ours == meta["abi"][tag]
+
+
+def test_ctypes_structs_match_header(xg, golden):
+    meta, _ = golden
+    abi = meta["abi"]["plain"]
+    assert ctypes.sizeof(xg.XGPUInfo) == abi["sizeof.XGPUInfo"]
+    assert ctypes.sizeof(xg.XGPUContext) == abi["sizeof.XGPUContext"]
+    for f, _ in xg.XGPUInfo._fields_:
+        assert getattr(xg.XGPUInfo, f).offset == abi[f"XGPUInfo.{f}"]
+    for f, _ in xg.XGPUContext._fields_:
+        assert getattr(xg.XGPUContext, f).offset == abi[f"XGPUContext.{f}"]
+
+
+def test_default_info(xg):
+    i = xg.default_info()
+    assert (i.npol, i.nstation, i.nfrequency, i.ntime, i.ntimepipe) == (2, 256, 10, 1024, 128)
+    assert i.nbaseline == 256 * 257 // 2
+    assert i.vecLength == 10 * 1024 * 256 * 2
+    assert i.vecLengthPipe == 10 * 128 * 256 * 2
+    # register-tile order by default, as xgpu_info.h:68-74
+    assert i.matrix_order == xg.REGISTER_TILE_TRIANGULAR_ORDER
+    assert i.matLength == 10 * (256 // 2 + 1) * (256 // 4) * 16
+    assert i.triLength == 10 * (256 * 257 // 2) * 4
+    assert "xgpu-b200" in xg.version()
+
+
+def test_random_complex_matches_reference(xg, golden):
+    _, arr = golden
+    ref = arr["s16_random_complex_seed1"]
+    libc = ctypes.CDLL(None)
+    libc.srand(1)
+    out = np.zeros(ref.size, dtype=np.int8)
+    xg.lib().xgpuRandomComplex(out.ctypes.data, ref.size // 2)
+    assert np.array_equal(out, ref)
+
+
+def test_reorder_matches_oracle_at_default_size(xg, oracle_mod):
+    i = xg.default_info()
+    n, f = i.nstation, i.nfrequency
+    rng = np.random.default_rng(5)
+    tri = rng.integers(-2**31, 2**31 - 1, size=i.triLength * 2, dtype=np.int64).astype(np.int32)
+    m = oracle_mod.tri_to_order(tri, n, f, 3000)
+    buf = m.copy()
+    xg.lib().xgpuReorderMatrix(buf.ctypes.data)
+    assert np.array_equal(buf[: tri.size], tri)
+    assert np.array_equal(buf[: tri.size], oracle_mod.reorder(m, n, f, 3000)[: tri.size])
+
+
+def test_swizzle_extract_omp_at_default_size(xg, oracle_mod):
+    i = xg.default_info()
+    n, f, t = i.nstation, i.nfrequency, i.ntime
+    x = oracle_mod.gaussian_input(n, f, t, seed=21)
+    sw = np.zeros_like(x)
+    xg.lib().xgpuSwizzleInput(sw.ctypes.data, x.ctypes.data)
+    assert np.array_equal(sw, oracle_mod.swizzle(x, n, f, t))
+    omp = np.zeros(i.triLength * 2, dtype=np.float32)
+    xg.lib().xgpuOmpXengine(omp.ctypes.data, x.ctypes.data)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    assert np.array_equal(omp, exact.astype(np.float32))
+    full = np.zeros(f * n * n * 8, dtype=np.float32)
+    xg.lib().xgpuExtractMatrix(full.ctypes.data, omp.ctypes.data)
+    assert np.array_equal(full, oracle_mod.extract_f32(omp, n, f))
+
+
+def test_check_result_reports(xg, capfd):
+    i = xg.default_info()
+    a = np.zeros(i.triLength * 2, dtype=np.float32)
+    b = a.copy()
+    xg.lib().xgpuCheckResult(a.ctypes.data, b.ctypes.data, 0, None)
+    assert "successful" in capfd.readouterr().out
+    a[10] = 5.0
+    xg.lib().xgpuCheckResult(a.ctypes.data, b.ctypes.data, 0, None)
+    assert "failed with 1 deviations" in capfd.readouterr().out
+
+
+def _ctx(xg):
+    return xg.XGPUContext()
+
+
+def test_errors_before_init(xg):
+    L = xg.lib()
+    ctx = _ctx(xg)
+    p = ctypes.byref(ctx)
+    assert L.xgpuCudaXengine(p, xg.SYNCOP_DUMP) == xg.XGPU_NOT_INITIALIZED
+    assert L.xgpuClearDeviceIntegrationBuffer(p) == xg.XGPU_NOT_INITIALIZED
+    assert L.xgpuSetHostInputBuffer(p) == xg.XGPU_NOT_INITIALIZED
+    assert L.xgpuSetHostOutputBuffer(p) == xg.XGPU_NOT_INITIALIZED
+    assert L.xgpuDumpDeviceIntegrationBuffer(p) == xg.XGPU_NOT_INITIALIZED
+    assert L.xgpuCudaXengineDevice(p, None, 0) == xg.XGPU_NOT_INITIALIZED
+    L.xgpuFree(p)
+    L.xgpuFree(p)  # idempotent, as cuda_xengine.cu:537
+
+
+@pytest.mark.parametrize("field,value", [
+    ("nstation", 24), ("nstation", 0), ("nfrequency", 0), ("ntimepipe", 8),
+    ("ntime", 100), ("compute_type", 7), ("output_type", 0), ("matrix_order", 1234),
+    ("engine", 9), ("input_format", 5),
+])
+def test_invalid_config_rejected_before_any_device_call(xg, field, value):
+    cfg = xg.default_config()
+    setattr(cfg, field, value)
+    ctx = _ctx(xg)
+    assert xg.lib().xgpuInitEx(ctypes.byref(ctx), 0, ctypes.byref(cfg)) == xg.XGPU_INVALID_ARGUMENT
+    assert not ctx.internal
+
+
+def test_tensor_engine_needs_integer_compute(xg):
+    cfg = xg.default_config()
+    cfg.engine = xg.XGPU_ENGINE_TENSOR
+    cfg.compute_type = xg.XGPU_FLOAT32
+    ctx = _ctx(xg)
+    assert xg.lib().xgpuInitEx(ctypes.byref(ctx), 0, ctypes.byref(cfg)) == xg.XGPU_INVALID_ARGUMENT
+
+
+def test_init_without_device_returns_error_not_exit(xg):
+    """xGPU calls exit(-1) with no device (cuda_xengine.cu:208-213); this
+    library returns XGPU_CUDA_ERROR.  Runs in a child so a GPU host still
+    exercises the no-device path (CUDA_VISIBLE_DEVICES empty)."""
+    code = (
+        "import ctypes, sys; sys.path.insert(0, %r); import xgpu_b200 as xg;"
+        "ctx = xg.XGPUContext();"
+        "r = xg.lib().xgpuInit(ctypes.byref(ctx), 0);"
+        "print('RC', r, bool(ctx.internal))" % ROOT)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run(["python", "-c", code], capture_output=True, text=True, env=env,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "RC 2 False" in out.stdout

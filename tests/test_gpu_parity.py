@@ -1,0 +1,253 @@
+"""Parity of libxgpu.so on a B200 against the oracle, through the C ABI.
+
+Integer engines (tcgen05 tensor cores, CUDA-core dp4a) must be bit-exact with
+the oracle's int64 sums, which tests/test_oracle_golden.py pins to the
+reference's xgpuOmpXengine.  The FP32 engine must equal the reference's float
+engine exactly where every partial sum is an integer below 2^24 (the
+configurations below), and stay within 1e-6 relative of the exact sums
+otherwise.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ENGINES = [("tensor", "int8"), ("plain", "int8"), ("plain", "fp32")]
+
+
+def correlate(xg, chunks, n, f, t, engine, compute, output="int32", order="tri", **kw):
+    """Run one integration of len(chunks) calls through xgpuCudaXengine."""
+    with xg.Correlator(n, f, t, engine=engine, compute=compute, output=output, order=order,
+                       **kw) as c:
+        for q, x in enumerate(chunks):
+            c.set_input(x)
+            c.run(xg.SYNCOP_DUMP if q == len(chunks) - 1 else xg.SYNCOP_NONE)
+        out = c.output_view()[: c.info.matLength * 2].copy()
+        exact = c.dump_int64() if compute == "int8" else None
+    return out, exact
+
+
+def expected_words(oracle_mod, exact, n, f, order, output):
+    words = exact.astype(np.int32) if output == "int32" else exact.astype(np.float32)
+    if order == "tri":
+        return words
+    code = {"ri": 2000, "rt": 3000}[order]
+    return oracle_mod.tri_to_order(words, n, f, code)
+
+
+@pytest.mark.parametrize("engine,compute", ENGINES)
+@pytest.mark.parametrize("n,f,t", [(16, 2, 64), (32, 3, 256), (48, 2, 128), (64, 10, 1024),
+                                   (80, 1, 512), (256, 10, 1024)])
+def test_single_call_triangular(xg, oracle_mod, engine, compute, n, f, t):
+    x = oracle_mod.gaussian_input(n, f, t, seed=n + f + t, sigma=16.0)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    output = "int32" if compute == "int8" else "float32"
+    out, ex64 = correlate(xg, [x], n, f, t, engine, compute, output=output)
+    if compute == "int8":
+        assert np.array_equal(ex64, exact)
+        assert np.array_equal(out, exact.astype(np.int32))
+    else:
+        assert np.array_equal(out, oracle_mod.xengine_f32(x, n, f, t))
+
+
+@pytest.mark.parametrize("engine,compute", ENGINES)
+@pytest.mark.parametrize("order", ["tri", "ri", "rt"])
+@pytest.mark.parametrize("output", ["int32", "float32"])
+def test_orders_and_output_types(xg, oracle_mod, engine, compute, order, output):
+    n, f, t = 32, 3, 256
+    x = oracle_mod.gaussian_input(n, f, t, seed=77, sigma=20.0)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    out, _ = correlate(xg, [x], n, f, t, engine, compute, output=output, order=order)
+    assert np.array_equal(out, expected_words(oracle_mod, exact, n, f, order, output))
+
+
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_reference_shapes_against_reference_digests(xg, oracle_mod, golden, engine):
+    """Configs 1-2 (N=64/256, F=10, T=1024): the dumped int32 triangular matrix
+    hashes to the reference xgpuOmpXengine DP4A output's digest."""
+    import hashlib
+    meta, _ = golden
+    for shape in ("c1", "c2"):
+        e = meta["shapes"][shape]
+        x = oracle_mod.gaussian_input(e["n"], e["f"], e["t"], seed=e["seed"], sigma=e["sigma"])
+        out, _ = correlate(xg, [x], e["n"], e["f"], e["t"], engine, "int8")
+        assert hashlib.sha256(out.tobytes()).hexdigest() == e["omp_dp4a_sha"], shape
+
+
+def test_fp32_reference_digest(xg, oracle_mod, golden):
+    import hashlib
+    meta, _ = golden
+    for shape in ("c1", "c2"):
+        e = meta["shapes"][shape]
+        x = oracle_mod.gaussian_input(e["n"], e["f"], e["t"], seed=e["seed"], sigma=e["sigma"])
+        out, _ = correlate(xg, [x], e["n"], e["f"], e["t"], "plain", "fp32", output="float32")
+        assert hashlib.sha256(out.tobytes()).hexdigest() == e["omp_fp32_sha"], shape
+
+
+@pytest.mark.parametrize("engine,compute", ENGINES)
+def test_multi_call_integration_and_clear(xg, oracle_mod, engine, compute):
+    n, f, t = 48, 4, 256
+    xs = [oracle_mod.gaussian_input(n, f, t, seed=s) for s in (1, 2, 3)]
+    output = "int32" if compute == "int8" else "float32"
+    with xg.Correlator(n, f, t, engine=engine, compute=compute, output=output) as c:
+        # Each syncOp once; the host buffer is rewritten only after a call that
+        # waited for its transfer (SYNC_TRANSFER / SYNC_COMPUTE), and the last
+        # call (SYNCOP_NONE) is completed by xgpuDumpDeviceIntegrationBuffer.
+        for x, sync in zip(xs, (xg.SYNCOP_SYNC_TRANSFER, xg.SYNCOP_SYNC_COMPUTE, xg.SYNCOP_NONE)):
+            c.set_input(x)
+            c.run(sync)
+        got = c.dump()
+        exact = oracle_mod.xengine_i64(np.concatenate(xs), n, f, 3 * t)
+        assert np.array_equal(got, exact.astype(got.dtype))
+        # clear starts a new integration
+        c.clear()
+        assert not c.dump().any()
+        c.set_input(xs[0])
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2]
+        assert np.array_equal(got, oracle_mod.xengine_i64(xs[0], n, f, t).astype(got.dtype))
+
+
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_exact_past_int32(xg, oracle_mod, engine):
+    """Full-scale -128 input for 3 x 32768 samples: every auto-correlation real
+    part is 3 * 32768 * 32768 = 3.2e9 > 2^31.  The int64 dump is exact; the
+    int32 dump wraps exactly as xGPU's int32 buffer would."""
+    n, f, t = 16, 1, 32768
+    x = np.full(t * f * n * 4, -128, dtype=np.int8)
+    x[1::4] = 127   # make the imaginary parts non-trivial
+    with xg.Correlator(n, f, t, ntimepipe=128, engine=engine) as c:
+        c.set_input(x)
+        for _ in range(2):
+            c.run(xg.SYNCOP_SYNC_COMPUTE)
+        c.run(xg.SYNCOP_DUMP)
+        ex = c.dump_int64()
+        out = c.output_view()[: c.info.matLength * 2].copy()
+    one = oracle_mod.xengine_i64(x, n, f, t)
+    want = 3 * one
+    assert np.abs(want).max() > 2**31
+    assert np.array_equal(ex, want)
+    assert np.array_equal(out, want.astype(np.int32))
+
+
+@pytest.mark.parametrize("engine,compute", ENGINES)
+def test_full_range_and_known_answers(xg, oracle_mod, golden, engine, compute):
+    _, arr = golden
+    n, f, t = 16, 2, 64
+    x = arr["s16_fullrange_input"]
+    out, _ = correlate(xg, [x], n, f, t, engine, compute,
+                       output="int32" if compute == "int8" else "float32")
+    want = arr["s16_fullrange_omp_dp4a"]
+    assert np.array_equal(out.astype(np.int64), want.astype(np.int64))
+    # known answer: only station 5 pol X non-zero, value (3 + 4j) at every sample
+    x = np.zeros(t * f * n * 4, dtype=np.int8).reshape(t, f, n, 2, 2)
+    x[:, :, 5, 0, 0] = 3
+    x[:, :, 5, 0, 1] = 4
+    out, _ = correlate(xg, [x.ravel()], n, f, t, engine, compute,
+                       output="int32" if compute == "int8" else "float32")
+    v = out.reshape(f, n * (n + 1) // 2, 2, 2, 2).astype(np.int64)
+    k55 = 5 * 6 // 2 + 5
+    assert (v[:, k55, 0, 0, 0] == 25 * t).all() and (v[:, k55, 0, 0, 1] == 0).all()
+    v[:, k55, 0, 0, 0] = 0
+    assert not v.any()
+
+
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_packed4_input(xg, oracle_mod, engine):
+    """4+4-bit packed input (one byte per complex sample) expands exactly."""
+    n, f, t = 64, 3, 512
+    packed = oracle_mod.generate(t * f * n * 2, 1, 2)
+    x = oracle_mod.unpack4(packed)
+    with xg.Correlator(n, f, t, engine=engine, input_format="packed4") as c:
+        c.set_input(packed)
+        c.run(xg.SYNCOP_DUMP)
+        ex = c.dump_int64()
+    assert np.array_equal(ex, oracle_mod.xengine_i64(x, n, f, t))
+
+
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_dp4a_swizzled_input(xg, oracle_mod, engine):
+    n, f, t = 32, 2, 256
+    x = oracle_mod.gaussian_input(n, f, t, seed=8)
+    with xg.Correlator(n, f, t, engine=engine, input_format="dp4a_swizzled") as c:
+        c.set_input(oracle_mod.swizzle(x, n, f, t))
+        c.run(xg.SYNCOP_DUMP)
+        ex = c.dump_int64()
+    assert np.array_equal(ex, oracle_mod.xengine_i64(x, n, f, t))
+
+
+def test_device_generator_matches_host(xg, oracle_mod):
+    import torch
+    for kind, sigma in [(0, 16.0), (0, 40.0), (1, 0.0), (2, 0.0)]:
+        nbytes = 1 << 20 | 3
+        d = torch.empty(nbytes, dtype=torch.int8, device="cuda")
+        xg.generate_device(d.data_ptr(), nbytes, kind, 1234, sigma)
+        assert np.array_equal(d.cpu().numpy(), oracle_mod.generate(nbytes, kind, 1234, sigma))
+
+
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_device_input_and_offsets(xg, oracle_mod, engine):
+    import torch
+    n, f, t = 64, 2, 256
+    x = oracle_mod.gaussian_input(n, f, t, seed=5)
+    d = torch.from_numpy(x).cuda()
+    with xg.Correlator(n, f, t, engine=engine) as c:
+        c.run_device(d.data_ptr(), xg.SYNCOP_SYNC_COMPUTE)
+        got = c.dump()
+        assert np.array_equal(got, oracle_mod.xengine_i64(x, n, f, t).astype(np.int32))
+
+
+def test_caller_buffers_registered_and_offsets(xg, oracle_mod):
+    """Caller-allocated host buffers (registered page-rounded, or not at all)
+    and input/output offsets, as xgpu.h:103-109 describes."""
+    n, f, t = 32, 2, 128
+    x = oracle_mod.gaussian_input(n, f, t, seed=6)
+    exact = oracle_mod.xengine_i64(x, n, f, t).astype(np.int32)
+    for flags in (0, xg.XGPU_DONT_REGISTER):
+        cfg = xg.default_config()
+        cfg.nstation, cfg.nfrequency, cfg.ntime, cfg.ntimepipe = n, f, t, 128
+        cfg.output_type, cfg.matrix_order = xg.XGPU_INT32, xg.TRIANGULAR_ORDER
+        off_in, off_out = 100, 7
+        inbuf = np.zeros(x.size + 2 * off_in + 64, dtype=np.int8)
+        inbuf[2 * off_in: 2 * off_in + x.size] = x
+        outbuf = np.zeros(2 * (exact.size // 2 + off_out) + 16, dtype=np.int32)
+        ctx = xg.XGPUContext()
+        ctx.array_h = inbuf.ctypes.data
+        ctx.array_len = inbuf.size // 2
+        ctx.matrix_h = outbuf.ctypes.data
+        ctx.matrix_len = outbuf.size // 2
+        L = xg.lib()
+        assert L.xgpuInitEx(ctypes.byref(ctx), flags, ctypes.byref(cfg)) == 0
+        if flags:
+            assert L.xgpuCudaXengine(ctypes.byref(ctx), 1) == xg.XGPU_HOST_BUFFER_NOT_SET
+            assert L.xgpuSetHostInputBuffer(ctypes.byref(ctx)) == 0
+            assert L.xgpuSetHostOutputBuffer(ctypes.byref(ctx)) == 0
+        ctx.input_offset, ctx.output_offset = off_in, off_out
+        assert L.xgpuCudaXengine(ctypes.byref(ctx), xg.SYNCOP_DUMP) == 0
+        assert np.array_equal(outbuf[2 * off_out: 2 * off_out + exact.size], exact)
+        # an offset that runs past the caller's buffer is refused
+        ctx.input_offset = ctx.array_len
+        assert L.xgpuCudaXengine(ctypes.byref(ctx), 1) == xg.XGPU_INVALID_ARGUMENT
+        L.xgpuFree(ctypes.byref(ctx))
+        assert not ctx.internal
+
+
+def test_reference_api_default_context(xg, oracle_mod):
+    """The unmodified xGPU calling sequence (cuda_correlator.c:145-253) at the
+    default sizes: xgpuInit with library-allocated buffers, xgpuCudaXengine
+    with SYNCOP_DUMP, xgpuReorderMatrix, compare with the CPU engine."""
+    L = xg.lib()
+    info = xg.default_info()
+    ctx = xg.XGPUContext()
+    assert L.xgpuInit(ctypes.byref(ctx), 0) == 0
+    x = oracle_mod.gaussian_input(info.nstation, info.nfrequency, info.ntime, seed=1)
+    ctypes.memmove(ctx.array_h, x.ctypes.data, x.size)
+    assert L.xgpuCudaXengine(ctypes.byref(ctx), xg.SYNCOP_DUMP) == 0
+    m = np.frombuffer((ctypes.c_float * (2 * info.matLength)).from_address(ctx.matrix_h),
+                      dtype=np.float32).copy()
+    L.xgpuReorderMatrix(m.ctypes.data)
+    exact = oracle_mod.xengine_i64(x, info.nstation, info.nfrequency, info.ntime)
+    assert np.array_equal(m[: exact.size], exact.astype(np.float32))
+    L.xgpuFree(ctypes.byref(ctx))

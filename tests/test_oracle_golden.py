@@ -1,0 +1,103 @@
+"""The oracle restatement against the reference's own outputs (CPU only).
+
+The fixtures in tests/golden were produced by the reference's CPU code
+(src/omp_xengine.c, src/cpu_util.c compiled per shape) on seeded inputs; see
+tests/golden/make_golden.py.  These tests pin the oracle before any GPU result
+is compared with it.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_generator_pins(oracle_mod, golden):
+    _, arr = golden
+    for kind, sigma in [(0, 16.0), (0, 40.0), (0, 4.0), (1, 0.0), (2, 0.0)]:
+        got = oracle_mod.generate(4096, kind, 7, sigma)
+        assert np.array_equal(got, arr[f"gen_k{kind}_s{int(sigma)}"]), (kind, sigma)
+
+
+@pytest.mark.parametrize("shape", ["s16", "s32"])
+def test_xengine_matches_reference_exactly(oracle_mod, golden, shape):
+    meta, arr = golden
+    e = meta["shapes"][shape]
+    n, f, t = e["n"], e["f"], e["t"]
+    x = oracle_mod.gaussian_input(n, f, t, seed=e["seed"], sigma=e["sigma"])
+    assert np.array_equal(x, arr[f"{shape}_input"])
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    # reference DP4A build: int32 words; its float sums are exact at this size
+    assert np.array_equal(exact, arr[f"{shape}_omp_dp4a"].astype(np.int64))
+    # reference float build, term for term
+    assert np.array_equal(oracle_mod.xengine_f32(x, n, f, t), arr[f"{shape}_omp_fp32"])
+
+
+@pytest.mark.parametrize("shape", ["c1", "c2"])
+def test_xengine_matches_reference_digest(oracle_mod, golden, shape):
+    """Configs 1 and 2 (N=64 and N=256, F=10, T=1024, sigma 16, seeds 0 and 1)."""
+    meta, _ = golden
+    e = meta["shapes"][shape]
+    n, f, t = e["n"], e["f"], e["t"]
+    x = oracle_mod.gaussian_input(n, f, t, seed=e["seed"], sigma=e["sigma"])
+    assert sha(x) == e["input_sha"]
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    assert sha(exact.astype(np.int32)) == e["omp_dp4a_sha"]
+    assert sha(exact.astype(np.float32)) == e["omp_fp32_sha"]
+
+
+def test_full_range_including_minus_128(oracle_mod, golden):
+    _, arr = golden
+    x = arr["s16_fullrange_input"]
+    n, f, t, _ = oracle_mod.REF_SHAPES["s16"]
+    assert (x == -128).sum() >= 64
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    assert np.array_equal(exact, arr["s16_fullrange_omp_dp4a"].astype(np.int64))
+
+
+@pytest.mark.parametrize("shape", ["s16", "s32"])
+@pytest.mark.parametrize("var,order", [("dp4a_rt", 3000), ("dp4a_ri", 2000),
+                                       ("fp32_rt", 3000), ("fp32_ri", 2000)])
+def test_orders_and_reorder(oracle_mod, golden, shape, var, order):
+    """Forward index maps of the three orders and the reference's reorder."""
+    meta, arr = golden
+    e = meta["shapes"][shape]
+    n, f = e["n"], e["f"]
+    words = arr[f"{shape}_omp_dp4a"] if var.startswith("dp4a") else arr[f"{shape}_omp_fp32"]
+    m = oracle_mod.tri_to_order(words, n, f, order)
+    assert np.array_equal(m, arr[f"{shape}_{var}_matrix"])
+    back = oracle_mod.reorder(m, n, f, order)[: words.size]
+    assert np.array_equal(back, arr[f"{shape}_{var}_reordered"])
+    assert np.array_equal(back, words)
+
+
+@pytest.mark.parametrize("shape", ["s16", "s32"])
+def test_swizzle_and_extract(oracle_mod, golden, shape):
+    meta, arr = golden
+    e = meta["shapes"][shape]
+    n, f, t = e["n"], e["f"], e["t"]
+    x = arr[f"{shape}_input"]
+    assert np.array_equal(oracle_mod.swizzle(x, n, f, t), arr[f"{shape}_swizzled"])
+    assert np.array_equal(oracle_mod.extract_f32(arr[f"{shape}_omp_fp32"], n, f),
+                          arr[f"{shape}_extract_fp32"])
+
+
+def test_oracle_accumulates(oracle_mod):
+    n, f, t = 16, 2, 64
+    a = oracle_mod.gaussian_input(n, f, t, seed=3)
+    b = oracle_mod.gaussian_input(n, f, t, seed=4)
+    acc = oracle_mod.xengine_i64(a, n, f, t)
+    oracle_mod.xengine_i64(b, n, f, t, acc=acc)
+    both = oracle_mod.xengine_i64(np.concatenate([a, b]), n, f, 2 * t)
+    assert np.array_equal(acc, both)
+
+
+def test_unpack4_roundtrip(oracle_mod):
+    p = oracle_mod.generate(4096, 1, 9)
+    u = oracle_mod.unpack4(p)
+    assert u.min() >= -7 and u.max() <= 7
+    repacked = ((u[0::2].astype(np.int32) & 0xF) << 4) | (u[1::2].astype(np.int32) & 0xF)
+    assert np.array_equal(repacked.astype(np.uint8), p.view(np.uint8))

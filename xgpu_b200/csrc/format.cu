@@ -1,0 +1,218 @@
+// format.cu -- device-side input conversion, output formatting and synthetic
+// input.
+//
+// Output orders (xgpu.h:45-47) are produced on the device from the triangular
+// integration buffer, so a dump copies exactly the requested layout to the
+// host.  The index maps follow the reference's writers and reorderers:
+//   TRIANGULAR_ORDER            kernel.cuh:96-117, cpu_util.c:161-162
+//   REAL_IMAG_TRIANGULAR_ORDER  kernel.cuh:72-95,  cpu_util.c:112-115
+//   REGISTER_TILE_...           kernel.cuh:49-71,  cpu_util.c:66-79
+#include <math.h>
+
+#include "internal.h"
+
+namespace xgpu {
+
+namespace fmt {
+
+struct Params {
+  const void *state;
+  int state_is_float;
+  int n, f;
+  long long nbaseline, mat_length;
+  int order, out_type;
+  uint32_t *out;  // matLength Complex = 2*matLength 32-bit words
+};
+
+__device__ __forceinline__ uint32_t convert(const void *state, int is_float, long long idx,
+                                            int out_type) {
+  if (is_float) {
+    const float v = ((const float *)state)[idx];
+    if (out_type == XGPU_INT32) return (uint32_t)__float2int_rn(v);
+    return __float_as_uint(v);
+  }
+  const long long v = ((const long long *)state)[idx];
+  if (out_type == XGPU_INT32) return (uint32_t)(unsigned long long)v;  // wraps like int32 sums
+  return __float_as_uint(__ll2float_rn(v));
+}
+
+// One thread per (channel, baseline, polarisation product).
+__global__ void format_kernel(const Params p) {
+  const long long total = (long long)p.f * p.nbaseline * 4;
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int pp = (int)(u & 3);
+    const long long fk = u >> 2;
+    const int f = (int)(fk / p.nbaseline);
+    const long long k = fk - (long long)f * p.nbaseline;
+    const uint32_t re = convert(p.state, p.state_is_float, 2 * u, p.out_type);
+    const uint32_t im = convert(p.state, p.state_is_float, 2 * u + 1, p.out_type);
+    if (p.order == TRIANGULAR_ORDER) {
+      *(uint2 *)(p.out + 2 * u) = make_uint2(re, im);
+    } else if (p.order == REAL_IMAG_TRIANGULAR_ORDER) {
+      p.out[u] = re;
+      p.out[u + p.mat_length] = im;
+    } else {
+      int i = (int)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
+      while ((long long)i * (i + 1) / 2 > k) --i;
+      while ((long long)(i + 1) * (i + 2) / 2 <= k) ++i;
+      const int j = (int)(k - (long long)i * (i + 1) / 2);
+      const long long rtn = (long long)(p.n / 2 + 1) * (p.n / 4);
+      const int I = i >> 1, J = j >> 1, rx = i & 1, ry = j & 1;
+      const long long l =
+          (long long)f * 4 * rtn + (long long)(2 * ry + rx) * rtn + (long long)I * (I + 1) / 2 + J;
+      const long long w = l * 4 + pp;
+      p.out[w] = re;
+      p.out[w + p.mat_length] = im;
+    }
+  }
+}
+
+// Packed 4+4-bit -> int8 pairs: 4 samples (one 32-bit word) per iteration.
+__global__ void unpack4_kernel(const uint32_t *in, uint2 *out, long long nwords) {
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nwords;
+       u += (long long)gridDim.x * blockDim.x) {
+    const uint32_t w = in[u];
+    uint32_t o[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t acc = 0;
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int byte = (int)((w >> (8 * (2 * h + b))) & 0xFF);
+        const int re = ((int)(int8_t)byte) >> 4;
+        const int im = ((int)(int8_t)(byte << 4)) >> 4;
+        acc |= ((uint32_t)(re & 0xFF) | ((uint32_t)(im & 0xFF) << 8)) << (16 * b);
+      }
+      o[h] = acc;
+    }
+    out[u] = make_uint2(o[0], o[1]);
+  }
+}
+
+// [t/4][f][s][p][c][t%4] -> [t][f][s][p][c] (inverse of cpu_util.c:235-255).
+__global__ void unswizzle_kernel(const uint32_t *in, int8_t *out, long long groups,
+                                 long long row_bytes) {
+  // groups = (t/4) * f * n * 4 entries of 4 bytes; row_bytes = f*n*4
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < groups;
+       u += (long long)gridDim.x * blockDim.x) {
+    const long long tq = u / row_bytes, e = u - tq * row_bytes;
+    const uint32_t w = in[u];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) out[(4 * tq + r) * row_bytes + e] = (int8_t)((w >> (8 * r)) & 0xFF);
+  }
+}
+
+// Seeded synthetic bytes; the same hash and tables as the host generator.
+struct GenParams {
+  uint32_t thr[254];
+  int kind;
+  unsigned long long seed;
+};
+
+__device__ __forceinline__ uint32_t hash32(unsigned long long seed, unsigned long long n) {
+  unsigned long long z = seed * 0x9E3779B97F4A7C15ull + n + 0x632BE59BD9B4E019ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (uint32_t)(z >> 32);
+}
+
+__device__ __forceinline__ int8_t gen_byte(const GenParams &g, const uint32_t *thr,
+                                           unsigned long long n) {
+  const uint32_t u = hash32(g.seed, n);
+  if (g.kind == 0) {
+    int lo = 0, hi = 254;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (u < thr[mid]) hi = mid; else lo = mid + 1;
+    }
+    return (int8_t)(lo - 127);
+  } else if (g.kind == 1) {
+    const uint32_t v = hash32(g.seed ^ 0x5A5A5A5A5A5A5A5Aull, n);
+    const int re = (int)(((unsigned long long)u * 15u) >> 32) - 7;
+    const int im = (int)(((unsigned long long)v * 15u) >> 32) - 7;
+    return (int8_t)(((re & 0xF) << 4) | (im & 0xF));
+  }
+  return (int8_t)((int)(((unsigned long long)u * 15u) >> 32) - 7);
+}
+
+__global__ void generate_kernel(int8_t *out, unsigned long long nbytes, const GenParams g) {
+  __shared__ uint32_t thr[254];
+  for (int q = threadIdx.x; q < 254; q += blockDim.x) thr[q] = g.thr[q];
+  __syncthreads();
+  const unsigned long long nwords = nbytes / 4;
+  for (unsigned long long w = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       w < nwords; w += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) v |= (uint32_t)(uint8_t)gen_byte(g, thr, 4 * w + b) << (8 * b);
+    ((uint32_t *)out)[w] = v;
+  }
+  if (blockIdx.x == 0)
+    for (unsigned long long n = nwords * 4 + threadIdx.x; n < nbytes; n += blockDim.x)
+      out[n] = gen_byte(g, thr, n);
+}
+
+static unsigned grid_for(long long work, int threads) {
+  long long b = (work + threads - 1) / threads;
+  if (b > 148LL * 16) b = 148LL * 16;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+}  // namespace fmt
+
+cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s, int order,
+                          int out_type, void *out, cudaStream_t st) {
+  if (order == REGISTER_TILE_TRIANGULAR_ORDER) {
+    // Slots that hold no baseline (kernel.cuh:65-71) stay zero.
+    cudaError_t e = cudaMemsetAsync(out, 0, (size_t)s.mat_length * 8, st);
+    if (e != cudaSuccess) return e;
+  }
+  fmt::Params p{state, state_is_float, s.n, s.f, s.nbaseline, s.mat_length, order, out_type,
+                (uint32_t *)out};
+  const long long work = (long long)s.f * s.nbaseline * 4;
+  fmt::format_kernel<<<fmt::grid_for(work, 256), 256, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack4(const uint8_t *in, int8_t *out, long long nsamples, cudaStream_t st) {
+  const long long nwords = nsamples / 4;  // nsamples is a multiple of 8 (n % 16 == 0)
+  fmt::unpack4_kernel<<<fmt::grid_for(nwords, 256), 256, 0, st>>>((const uint32_t *)in,
+                                                                  (uint2 *)out, nwords);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unswizzle_dp4a(const int8_t *in, int8_t *out, const Sizes &s,
+                                  cudaStream_t st) {
+  const long long row_bytes = (long long)s.f * s.n * 4;
+  const long long groups = (long long)(s.t / 4) * row_bytes;
+  fmt::unswizzle_kernel<<<fmt::grid_for(groups, 256), 256, 0, st>>>((const uint32_t *)in, out,
+                                                                    groups, row_bytes);
+  return cudaGetLastError();
+}
+
+void gauss_thresholds(double sigma, uint32_t thr[254]) {
+  for (int k = -127; k < 127; k++) {
+    double pr = 0.5 * erfc(-((k + 0.5) / sigma) / sqrt(2.0));
+    double sc = floor(pr * 4294967296.0);
+    if (sc > 4294967295.0) sc = 4294967295.0;
+    if (sc < 0) sc = 0;
+    thr[k + 127] = (uint32_t)sc;
+  }
+}
+
+cudaError_t launch_generate(void *out, size_t nbytes, int kind, unsigned long long seed,
+                            double sigma, cudaStream_t st) {
+  fmt::GenParams g;
+  g.kind = kind;
+  g.seed = seed;
+  if (kind == 0) gauss_thresholds(sigma, g.thr);
+  else for (int q = 0; q < 254; ++q) g.thr[q] = 0;
+  fmt::generate_kernel<<<fmt::grid_for((long long)(nbytes / 4) + 1, 256), 256, 0, st>>>(
+      (int8_t *)out, (unsigned long long)nbytes, g);
+  return cudaGetLastError();
+}
+
+}  // namespace xgpu

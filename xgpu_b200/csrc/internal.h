@@ -1,0 +1,76 @@
+// internal.h -- state and launcher interfaces shared by the libxgpu.so sources.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/xgpu.h"
+
+namespace xgpu {
+
+constexpr int kNpol = 2;
+
+// Samples per launch of an integer engine.  An int32 partial sum of one launch
+// holds at most 2 * 128 * 128 * kSegment = 2^30 in magnitude (both products of
+// a real or imaginary part at full scale -128), so the int32 accumulators stay
+// exact; each launch adds into the int64 integration buffer.
+constexpr int kSegment = 32768;
+
+// Device error codes written by kernels into the context's error word.
+enum DeviceError : int {
+  kErrNone = 0,
+  kErrTimeoutProducer = 1,   // TMA producer gave up waiting for a free stage
+  kErrTimeoutMma = 2,        // MMA issuer gave up waiting for a loaded stage
+  kErrTimeoutDrain = 3,      // epilogue gave up waiting for the accumulator
+};
+
+struct Sizes {
+  int n;       // stations
+  int f;       // channels
+  int t;       // samples per call
+  int tp;      // samples per transfer chunk
+  long long nbaseline;   // n(n+1)/2
+  long long vec_length;  // ComplexInput elements per call = t*f*n*2
+  long long input_bytes; // bytes of one call's input in its format
+  long long mat_length;  // Complex elements of a dump in the context's order
+  long long tri_length;  // Complex elements in triangular order
+  long long state_elems; // int64 (or float) words of the integration buffer = tri_length*2
+};
+
+Sizes make_sizes(const XGPUConfig &cfg);
+
+// ---- engines --------------------------------------------------------------
+// All engines read int8 input laid out [t][f][s][p][c] (t = 0..t_total) and
+// add samples [t0, t0+tcount) into the triangular integration buffer
+// state[f][k][p1][p2][re,im], k = i(i+1)/2 + j, i >= j.  overwrite != 0
+// stores instead of adding (the buffer is known to be zero).
+
+cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
+                              int64_t *state, int overwrite, cudaStream_t st);
+cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount,
+                              float *state, int overwrite, cudaStream_t st);
+
+// Tensor-core engine.  The tensor map describes `in` (see make_tc_tensor_map).
+cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
+                      int64_t *state, int overwrite, int *err, cudaStream_t st);
+// Encodes the 3-D tensor map {x: 4n bytes, y: f, z: t} over a device input
+// buffer.  Returns 0 on success.
+int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);
+// 0 if the tensor-core kernel image loads on the current device.
+cudaError_t tc_check_device();
+
+// ---- input conversion, output formatting, synthetic input -----------------
+cudaError_t launch_unpack4(const uint8_t *in, int8_t *out, long long nsamples, cudaStream_t st);
+cudaError_t launch_unswizzle_dp4a(const int8_t *in, int8_t *out, const Sizes &s, cudaStream_t st);
+// state (int64 or float) -> Complex words in `order` of type out_type.
+cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s, int order,
+                          int out_type, void *out, cudaStream_t st);
+cudaError_t launch_generate(void *out, size_t nbytes, int kind, unsigned long long seed,
+                            double sigma, cudaStream_t st);
+
+// Host Gaussian table shared with the generator kernel.
+void gauss_thresholds(double sigma, uint32_t thr[254]);
+
+}  // namespace xgpu

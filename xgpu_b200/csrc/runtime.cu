@@ -1,0 +1,611 @@
+// runtime.cu -- the xgpu.h C ABI: contexts, host buffers, the per-call
+// pipeline and dumps.
+//
+// Counterpart of xGPU's src/cuda_xengine.cu (host side).  Differences by
+// design:
+//  * sizes are per context (xgpuInitEx) with the build's defaults for
+//    xgpuInit; all state lives in the context, so contexts are re-entrant
+//    (xGPU keeps textures as file-scope globals, cuda_xengine.cu:73-87);
+//  * a call copies its whole input with one host-to-device transfer into one
+//    of two device buffers and runs one engine launch over all its samples
+//    (xGPU launches once per NTIME_PIPE chunk and re-reads/writes the whole
+//    integration buffer each time, cuda_xengine.cu:599-653).  Consecutive
+//    calls still overlap: the transfer of call k+1 runs while call k computes;
+//  * the integer engines integrate into an int64 buffer, converted to the
+//    caller's Complex type and matrix order on the device at dump time;
+//  * xgpuClearDeviceIntegrationBuffer is lazy: the next engine launch stores
+//    instead of adding, so a cleared buffer is never read.
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include <mutex>
+#include <new>
+
+#include "internal.h"
+
+#ifndef NSTATION
+#define NSTATION 256
+#endif
+#ifndef NFREQUENCY
+#define NFREQUENCY 10
+#endif
+#ifndef NTIME
+#define NTIME 1024
+#endif
+#ifndef NTIME_PIPE
+#define NTIME_PIPE 128
+#endif
+#if defined MATRIX_ORDER_TRIANGULAR
+#define XGPU_DEFAULT_ORDER TRIANGULAR_ORDER
+#elif defined MATRIX_ORDER_REAL_IMAG
+#define XGPU_DEFAULT_ORDER REAL_IMAG_TRIANGULAR_ORDER
+#else
+#define XGPU_DEFAULT_ORDER REGISTER_TILE_TRIANGULAR_ORDER
+#endif
+#ifdef DP4A
+#define XGPU_DEFAULT_OUTPUT XGPU_INT32
+#else
+#define XGPU_DEFAULT_OUTPUT XGPU_FLOAT32
+#endif
+#ifndef XGPU_VERSION
+#define XGPU_VERSION "xgpu-b200-1.0"
+#endif
+
+using namespace xgpu;
+
+namespace {
+
+struct Internal {
+  int device = 0;
+  XGPUConfig cfg{};
+  Sizes sz{};
+  bool int_state = true;  // int64 buffer (integer engines) or float (FP32)
+
+  void *d_in[2] = {nullptr, nullptr};  // one call's input, as supplied
+  int8_t *d_conv = nullptr;            // int8 [t][f][s][p][c] after conversion
+  void *d_state = nullptr;             // integration buffer
+  void *d_out = nullptr;               // formatted dump
+  int *d_err = nullptr;                // device error word
+  int *h_err = nullptr;                // pinned copy of it
+
+  cudaStream_t s_copy = nullptr, s_comp = nullptr;
+  cudaStream_t s_own = nullptr;  // the context's own compute stream
+  cudaEvent_t copy_done[2] = {nullptr, nullptr};
+  cudaEvent_t comp_done[2] = {nullptr, nullptr};
+  int cur = 0;
+  bool state_zero = true;
+
+  // tensor maps, cached by device pointer
+  struct MapEntry {
+    const void *ptr;
+    CUtensorMap map;
+  } maps[4];
+  int nmaps = 0;
+
+  ComplexInput *free_array_h = nullptr, *unregister_array_h = nullptr;
+  bool array_h_set = false, register_host_array = true;
+  Complex *free_matrix_h = nullptr, *unregister_matrix_h = nullptr;
+  bool matrix_h_set = false, register_host_matrix = true;
+};
+
+const long kPageSize = sysconf(_SC_PAGE_SIZE);
+
+#define XGPU_CHECK(call)                                                               \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      fprintf(stderr, "(CUDA) %s (%s:%d)\n", cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return XGPU_CUDA_ERROR;                                                          \
+    }                                                                                  \
+  } while (0)
+
+Internal *get(XGPUContext *c) { return c ? (Internal *)c->internal : nullptr; }
+
+XGPUConfig default_config() {
+  XGPUConfig c;
+  c.nstation = NSTATION;
+  c.nfrequency = NFREQUENCY;
+  c.ntime = NTIME;
+  c.ntimepipe = NTIME_PIPE;
+  c.compute_type = XGPU_INT8;
+  c.output_type = XGPU_DEFAULT_OUTPUT;
+  c.matrix_order = XGPU_DEFAULT_ORDER;
+  c.engine = XGPU_ENGINE_TENSOR;
+  c.input_format = XGPU_INPUT_INT8;
+  return c;
+}
+
+int validate(const XGPUConfig &c) {
+  if (c.nstation < 16 || c.nstation % 16 != 0 || c.nstation > 8192) return 0;
+  if (c.nfrequency < 1 || c.nfrequency > 65535) return 0;
+  if (c.ntimepipe < 16 || c.ntimepipe % 16 != 0) return 0;
+  if (c.ntime < c.ntimepipe || c.ntime % c.ntimepipe != 0) return 0;
+  if (c.compute_type != XGPU_INT8 && c.compute_type != XGPU_FLOAT32) return 0;
+  if (c.output_type != XGPU_INT32 && c.output_type != XGPU_FLOAT32) return 0;
+  if (c.matrix_order != TRIANGULAR_ORDER && c.matrix_order != REAL_IMAG_TRIANGULAR_ORDER &&
+      c.matrix_order != REGISTER_TILE_TRIANGULAR_ORDER)
+    return 0;
+  if (c.engine > XGPU_ENGINE_TENSOR) return 0;
+  if (c.engine == XGPU_ENGINE_TENSOR && c.compute_type != XGPU_INT8) return 0;
+  if (c.input_format > XGPU_INPUT_DP4A_SWIZZLED) return 0;
+  // input bytes of one call must fit the 32-bit sample index space of the engines
+  const double bytes = 4.0 * c.nstation * c.nfrequency * (double)c.ntime;
+  if (bytes > 1.0e12) return 0;
+  return 1;
+}
+
+void fill_info(const XGPUConfig &c, const Sizes &s, XGPUInfo *info) {
+  info->npol = kNpol;
+  info->nstation = c.nstation;
+  info->nbaseline = (unsigned)s.nbaseline;
+  info->nfrequency = c.nfrequency;
+  info->ntime = c.ntime;
+  info->ntimepipe = c.ntimepipe;
+  info->input_type = XGPU_INT8;
+  info->compute_type = c.compute_type;
+  info->vecLength = (unsigned long long)s.vec_length;
+  info->vecLengthPipe = (unsigned long long)c.nfrequency * c.ntimepipe * c.nstation * kNpol;
+  info->matLength = (unsigned long long)s.mat_length;
+  info->triLength = (unsigned long long)s.tri_length;
+  info->matrix_order = c.matrix_order;
+  info->shared_atomic_size = 4;
+  info->complex_block_size = 1;
+}
+
+int free_device(Internal *in) {
+  cudaSetDevice(in->device);
+  if (in->s_copy) cudaStreamSynchronize(in->s_copy);
+  if (in->s_comp) cudaStreamSynchronize(in->s_comp);
+  for (int b = 0; b < 2; ++b) {
+    if (in->copy_done[b]) cudaEventDestroy(in->copy_done[b]);
+    if (in->comp_done[b]) cudaEventDestroy(in->comp_done[b]);
+    if (in->d_in[b]) cudaFree(in->d_in[b]);
+  }
+  if (in->s_copy) cudaStreamDestroy(in->s_copy);
+  if (in->s_own) cudaStreamDestroy(in->s_own);
+  if (in->d_conv) cudaFree(in->d_conv);
+  if (in->d_state) cudaFree(in->d_state);
+  if (in->d_out) cudaFree(in->d_out);
+  if (in->d_err) cudaFree(in->d_err);
+  if (in->h_err) cudaFreeHost(in->h_err);
+  return XGPU_OK;
+}
+
+// Register caller memory page-rounded, as cuda_xengine.cu:386-412 does.
+cudaError_t register_range(void *p, size_t bytes, void **registered) {
+  uintptr_t a = (uintptr_t)p, base = a - (a % kPageSize);
+  size_t len = bytes + (a - base);
+  len = (len + kPageSize - 1) / kPageSize * kPageSize;
+  cudaError_t e = cudaHostRegister((void *)base, len, cudaHostRegisterDefault);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {
+    cudaGetLastError();
+    *registered = nullptr;  // someone else owns the registration
+    return cudaSuccess;
+  }
+  *registered = (e == cudaSuccess) ? (void *)base : nullptr;
+  return e;
+}
+
+const CUtensorMap *tensor_map(Internal *in, const void *ptr) {
+  for (int q = 0; q < in->nmaps; ++q)
+    if (in->maps[q].ptr == ptr) return &in->maps[q].map;
+  const int slot = in->nmaps < 4 ? in->nmaps++ : 3;
+  if (make_tc_tensor_map(&in->maps[slot].map, ptr, in->sz) != 0) {
+    in->maps[slot].ptr = nullptr;
+    return nullptr;
+  }
+  in->maps[slot].ptr = ptr;
+  return &in->maps[slot].map;
+}
+
+// Queue the engine over one call's device input (any format) on s_comp.
+int run_engine(Internal *in, const void *d_input) {
+  const Sizes &s = in->sz;
+  const int8_t *x = (const int8_t *)d_input;
+  if (in->cfg.input_format == XGPU_INPUT_PACKED4) {
+    XGPU_CHECK(launch_unpack4((const uint8_t *)d_input, in->d_conv, s.vec_length, in->s_comp));
+    x = in->d_conv;
+  } else if (in->cfg.input_format == XGPU_INPUT_DP4A_SWIZZLED) {
+    XGPU_CHECK(launch_unswizzle_dp4a((const int8_t *)d_input, in->d_conv, s, in->s_comp));
+    x = in->d_conv;
+  }
+  const int ow = in->state_zero ? 1 : 0;
+  if (!in->int_state) {
+    XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp));
+  } else if (in->cfg.engine == XGPU_ENGINE_PLAIN) {
+    for (int t0 = 0; t0 < s.t; t0 += kSegment) {
+      const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
+      XGPU_CHECK(launch_plain_dp4a(x, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
+                                   in->s_comp));
+    }
+  } else {
+    const CUtensorMap *map = tensor_map(in, x);
+    if (!map) {
+      fprintf(stderr, "xgpu: cannot describe the input buffer to the tensor memory accelerator\n");
+      return XGPU_CUDA_ERROR;
+    }
+    for (int t0 = 0; t0 < s.t; t0 += kSegment) {
+      const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
+      XGPU_CHECK(launch_tc(*map, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0, in->d_err,
+                           in->s_comp));
+    }
+  }
+  in->state_zero = false;
+  return XGPU_OK;
+}
+
+// Read and clear the device error word; s_comp must be idle.
+int check_device_error(Internal *in) {
+  XGPU_CHECK(cudaMemcpyAsync(in->h_err, in->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                             in->s_comp));
+  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  if (*in->h_err != 0) {
+    fprintf(stderr, "xgpu: device wait timed out (code %d); results of this integration are invalid\n",
+            *in->h_err);
+    XGPU_CHECK(cudaMemsetAsync(in->d_err, 0, sizeof(int), in->s_comp));
+    XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+    return XGPU_CUDA_ERROR;
+  }
+  return XGPU_OK;
+}
+
+int dump(XGPUContext *ctx, Internal *in) {
+  if (!in->matrix_h_set || !ctx->matrix_h) return XGPU_HOST_BUFFER_NOT_SET;
+  if (ctx->matrix_len && ctx->output_offset + (size_t)in->sz.mat_length > ctx->matrix_len)
+    return XGPU_INVALID_ARGUMENT;
+  if (in->state_zero) {
+    XGPU_CHECK(cudaMemsetAsync(in->d_state, 0, (size_t)in->sz.state_elems * (in->int_state ? 8 : 4),
+                               in->s_comp));
+  }
+  XGPU_CHECK(launch_format(in->d_state, in->int_state ? 0 : 1, in->sz, in->cfg.matrix_order,
+                           in->cfg.output_type, in->d_out, in->s_comp));
+  XGPU_CHECK(cudaMemcpyAsync(ctx->matrix_h + ctx->output_offset, in->d_out,
+                             (size_t)in->sz.mat_length * sizeof(Complex), cudaMemcpyDeviceToHost,
+                             in->s_comp));
+  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  return check_device_error(in);
+}
+
+int finish_call(XGPUContext *ctx, Internal *in, int syncOp) {
+  switch (syncOp) {
+    case SYNCOP_DUMP:
+      return dump(ctx, in);
+    case SYNCOP_SYNC_TRANSFER:
+      XGPU_CHECK(cudaStreamSynchronize(in->s_copy));
+      return XGPU_OK;
+    case SYNCOP_SYNC_COMPUTE:
+      XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+      return check_device_error(in);
+    default:
+      return XGPU_OK;
+  }
+}
+
+}  // namespace
+
+namespace xgpu {
+
+Sizes make_sizes(const XGPUConfig &c) {
+  Sizes s;
+  s.n = (int)c.nstation;
+  s.f = (int)c.nfrequency;
+  s.t = (int)c.ntime;
+  s.tp = (int)c.ntimepipe;
+  s.nbaseline = (long long)s.n * (s.n + 1) / 2;
+  s.vec_length = (long long)s.t * s.f * s.n * kNpol;
+  s.input_bytes = c.input_format == XGPU_INPUT_PACKED4 ? s.vec_length : 2 * s.vec_length;
+  s.tri_length = (long long)s.f * s.nbaseline * kNpol * kNpol;
+  s.mat_length = c.matrix_order == REGISTER_TILE_TRIANGULAR_ORDER
+                     ? (long long)s.f * (s.n / 2 + 1) * (s.n / 4) * kNpol * kNpol * 4
+                     : s.tri_length;
+  s.state_elems = 2 * s.tri_length;
+  return s;
+}
+
+}  // namespace xgpu
+
+extern "C" {
+
+const char *xgpuVersionString() { return XGPU_VERSION " (sm_100a; engines: tcgen05-int8, dp4a, fp32)"; }
+
+void xgpuDefaultConfig(XGPUConfig *cfg) {
+  if (cfg) *cfg = default_config();
+}
+
+void xgpuInfo(XGPUInfo *pcxs) {
+  if (!pcxs) return;
+  XGPUConfig c = default_config();
+  fill_info(c, make_sizes(c), pcxs);
+}
+
+int xgpuContextInfo(XGPUContext *context, XGPUInfo *info) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  if (!info) return XGPU_INVALID_ARGUMENT;
+  fill_info(in->cfg, in->sz, info);
+  return XGPU_OK;
+}
+
+const char *xgpuEngineName(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return "none";
+  if (!in->int_state) return "plain-fp32";
+  return in->cfg.engine == XGPU_ENGINE_PLAIN ? "plain-dp4a" : "tensor-tcgen05-int8";
+}
+
+int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in) {
+  if (!context || !cfg_in) return XGPU_INVALID_ARGUMENT;
+  XGPUConfig cfg = *cfg_in;
+  if (cfg.engine == XGPU_ENGINE_DEFAULT)
+    cfg.engine = cfg.compute_type == XGPU_INT8 ? XGPU_ENGINE_TENSOR : XGPU_ENGINE_PLAIN;
+  if (!validate(cfg)) return XGPU_INVALID_ARGUMENT;
+
+  Internal *in = new (std::nothrow) Internal();
+  if (!in) return XGPU_OUT_OF_MEMORY;
+  context->internal = in;
+  in->device = device_flags & XGPU_DEVICE_MASK;
+  in->register_host_array = !(device_flags & XGPU_DONT_REGISTER_ARRAY);
+  in->register_host_matrix = !(device_flags & XGPU_DONT_REGISTER_MATRIX);
+  in->cfg = cfg;
+  in->sz = make_sizes(cfg);
+  in->int_state = cfg.compute_type == XGPU_INT8;
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    fprintf(stderr, "xgpu: no CUDA devices found\n");
+    delete in;
+    context->internal = nullptr;
+    return XGPU_CUDA_ERROR;
+  }
+  if (in->device >= ndev) {
+    delete in;
+    context->internal = nullptr;
+    return XGPU_INVALID_ARGUMENT;
+  }
+  auto fail = [&](int code) {
+    free_device(in);
+    delete in;
+    context->internal = nullptr;
+    return code;
+  };
+  if (cudaSetDevice(in->device) != cudaSuccess) return fail(XGPU_CUDA_ERROR);
+  if (cfg.engine == XGPU_ENGINE_TENSOR && tc_check_device() != cudaSuccess) {
+    cudaGetLastError();
+    fprintf(stderr, "xgpu: the tensor-core engine needs an sm_100 (B200-class) device\n");
+    return fail(XGPU_CUDA_ERROR);
+  }
+
+  const Sizes &s = in->sz;
+  const size_t in_bytes = (size_t)((s.input_bytes + 255) / 256 * 256);
+  const size_t state_bytes = (size_t)s.state_elems * (in->int_state ? 8 : 4);
+  if (cudaMalloc(&in->d_in[0], in_bytes) != cudaSuccess ||
+      cudaMalloc(&in->d_in[1], in_bytes) != cudaSuccess ||
+      cudaMalloc(&in->d_state, state_bytes) != cudaSuccess ||
+      cudaMalloc(&in->d_out, (size_t)s.mat_length * sizeof(Complex)) != cudaSuccess ||
+      cudaMalloc(&in->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&in->h_err, sizeof(int)) != cudaSuccess ||
+      (cfg.input_format != XGPU_INPUT_INT8 &&
+       cudaMalloc(&in->d_conv, (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess)) {
+    cudaGetLastError();
+    return fail(XGPU_OUT_OF_MEMORY);
+  }
+  if (cudaStreamCreateWithFlags(&in->s_copy, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&in->s_own, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(XGPU_CUDA_ERROR);
+  in->s_comp = in->s_own;
+  for (int b = 0; b < 2; ++b) {
+    if (cudaEventCreateWithFlags(&in->copy_done[b], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&in->comp_done[b], cudaEventDisableTiming) != cudaSuccess)
+      return fail(XGPU_CUDA_ERROR);
+  }
+  if (cudaMemsetAsync(in->d_err, 0, sizeof(int), in->s_comp) != cudaSuccess ||
+      cudaMemsetAsync(in->d_state, 0, state_bytes, in->s_comp) != cudaSuccess ||
+      cudaStreamSynchronize(in->s_comp) != cudaSuccess)
+    return fail(XGPU_CUDA_ERROR);
+  in->state_zero = true;
+
+  if (in->register_host_array) {
+    int r = xgpuSetHostInputBuffer(context);
+    if (r != XGPU_OK) return fail(r);
+  }
+  if (in->register_host_matrix) {
+    int r = xgpuSetHostOutputBuffer(context);
+    if (r != XGPU_OK) return fail(r);
+  }
+  return XGPU_OK;
+}
+
+int xgpuInit(XGPUContext *context, int device_flags) {
+  XGPUConfig cfg = default_config();
+  const char *e = getenv("XGPU_ENGINE");
+  if (e && strcmp(e, "plain") == 0) cfg.engine = XGPU_ENGINE_PLAIN;
+  if (e && strcmp(e, "fp32") == 0) {
+    cfg.engine = XGPU_ENGINE_PLAIN;
+    cfg.compute_type = XGPU_FLOAT32;
+  }
+  return xgpuInitEx(context, device_flags, &cfg);
+}
+
+int xgpuClearDeviceIntegrationBuffer(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  // Ordered after queued engine launches; the next launch overwrites.
+  in->state_zero = true;
+  return XGPU_OK;
+}
+
+int xgpuSetHostInputBuffer(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  XGPU_CHECK(cudaStreamSynchronize(in->s_copy));
+  if (in->free_array_h) {
+    cudaFreeHost(in->free_array_h);
+    in->free_array_h = nullptr;
+  }
+  if (in->unregister_array_h) {
+    cudaHostUnregister(in->unregister_array_h);
+    in->unregister_array_h = nullptr;
+  }
+  in->array_h_set = true;
+  if (context->array_h) {
+    if (in->register_host_array) {
+      void *reg = nullptr;
+      XGPU_CHECK(register_range(context->array_h, context->array_len * sizeof(ComplexInput), &reg));
+      in->unregister_array_h = (ComplexInput *)reg;
+    }
+  } else {
+    const size_t bytes = (size_t)in->sz.input_bytes;
+    // array_len counts ComplexInput elements (2 bytes); packed input needs half.
+    context->array_len = (bytes + sizeof(ComplexInput) - 1) / sizeof(ComplexInput);
+    XGPU_CHECK(cudaMallocHost((void **)&context->array_h, context->array_len * sizeof(ComplexInput)));
+    in->free_array_h = context->array_h;
+  }
+  context->input_offset = 0;
+  return XGPU_OK;
+}
+
+int xgpuSetHostOutputBuffer(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  if (in->free_matrix_h) {
+    cudaFreeHost(in->free_matrix_h);
+    in->free_matrix_h = nullptr;
+  }
+  if (in->unregister_matrix_h) {
+    cudaHostUnregister(in->unregister_matrix_h);
+    in->unregister_matrix_h = nullptr;
+  }
+  in->matrix_h_set = true;
+  if (context->matrix_h) {
+    if (in->register_host_matrix) {
+      void *reg = nullptr;
+      XGPU_CHECK(register_range(context->matrix_h, context->matrix_len * sizeof(Complex), &reg));
+      in->unregister_matrix_h = (Complex *)reg;
+    }
+  } else {
+    context->matrix_len = (size_t)in->sz.mat_length;
+    XGPU_CHECK(cudaMallocHost((void **)&context->matrix_h, context->matrix_len * sizeof(Complex)));
+    in->free_matrix_h = context->matrix_h;
+  }
+  context->output_offset = 0;
+  return XGPU_OK;
+}
+
+void xgpuFree(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return;
+  cudaSetDevice(in->device);
+  if (in->s_copy) cudaStreamSynchronize(in->s_copy);
+  if (in->s_comp) cudaStreamSynchronize(in->s_comp);
+  if (in->free_array_h) {
+    cudaFreeHost(in->free_array_h);
+    context->array_h = nullptr;
+  }
+  if (in->unregister_array_h) {
+    cudaHostUnregister(in->unregister_array_h);
+    context->array_h = nullptr;
+  }
+  if (in->free_matrix_h) {
+    cudaFreeHost(in->free_matrix_h);
+    context->matrix_h = nullptr;
+  }
+  if (in->unregister_matrix_h) {
+    cudaHostUnregister(in->unregister_matrix_h);
+    context->matrix_h = nullptr;
+  }
+  free_device(in);
+  delete in;
+  context->internal = nullptr;
+}
+
+int xgpuCudaXengine(XGPUContext *context, int syncOp) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  if (!in->array_h_set || !in->matrix_h_set) return XGPU_HOST_BUFFER_NOT_SET;
+  if (syncOp < SYNCOP_NONE || syncOp > SYNCOP_SYNC_COMPUTE) return XGPU_INVALID_ARGUMENT;
+  if (!context->array_h) return XGPU_HOST_BUFFER_NOT_SET;
+  const size_t need = (size_t)((in->sz.input_bytes + 1) / 2);  // in ComplexInput units
+  if (context->array_len && context->input_offset + need > context->array_len)
+    return XGPU_INVALID_ARGUMENT;
+  XGPU_CHECK(cudaSetDevice(in->device));
+
+  const int b = in->cur;
+  in->cur ^= 1;
+  // The buffer is free once the engine launch that last read it has finished.
+  XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
+  XGPU_CHECK(cudaMemcpyAsync(in->d_in[b], context->array_h + context->input_offset,
+                             (size_t)in->sz.input_bytes, cudaMemcpyHostToDevice, in->s_copy));
+  XGPU_CHECK(cudaEventRecord(in->copy_done[b], in->s_copy));
+  XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->copy_done[b], 0));
+  int r = run_engine(in, in->d_in[b]);
+  if (r != XGPU_OK) return r;
+  XGPU_CHECK(cudaEventRecord(in->comp_done[b], in->s_comp));
+  return finish_call(context, in, syncOp);
+}
+
+int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int syncOp) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  if (!device_input || ((uintptr_t)device_input & 15) != 0) return XGPU_INVALID_ARGUMENT;
+  if (syncOp < SYNCOP_NONE || syncOp > SYNCOP_SYNC_COMPUTE) return XGPU_INVALID_ARGUMENT;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  int r = run_engine(in, device_input);
+  if (r != XGPU_OK) return r;
+  return finish_call(context, in, syncOp);
+}
+
+int xgpuDumpDeviceIntegrationBuffer(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  return dump(context, in);
+}
+
+int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_out) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  if (!host_out || !in->int_state) return XGPU_INVALID_ARGUMENT;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  const size_t bytes = (size_t)in->sz.state_elems * 8;
+  if (in->state_zero) {
+    XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+    memset(host_out, 0, bytes);
+    return check_device_error(in);
+  }
+  XGPU_CHECK(cudaMemcpyAsync(host_out, in->d_state, bytes, cudaMemcpyDeviceToHost, in->s_comp));
+  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  return check_device_error(in);
+}
+
+int xgpuSetComputeStream(XGPUContext *context, void *stream) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  cudaStream_t next = stream ? (cudaStream_t)stream : in->s_own;
+  if (next == in->s_comp) return XGPU_OK;
+  // Order the new stream after everything queued on the old one.
+  cudaEvent_t ev;
+  XGPU_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  XGPU_CHECK(cudaEventRecord(ev, in->s_comp));
+  XGPU_CHECK(cudaStreamWaitEvent(next, ev, 0));
+  XGPU_CHECK(cudaEventDestroy(ev));
+  in->s_comp = next;
+  return XGPU_OK;
+}
+
+int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long long seed,
+                       double sigma, int device) {
+  if (!device_out || kind < 0 || kind > 2 || (kind == 0 && !(sigma > 0))) return XGPU_INVALID_ARGUMENT;
+  XGPU_CHECK(cudaSetDevice(device));
+  XGPU_CHECK(launch_generate(device_out, nbytes, kind, seed, sigma, 0));
+  XGPU_CHECK(cudaStreamSynchronize(0));
+  return XGPU_OK;
+}
+
+}  // extern "C"
