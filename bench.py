@@ -151,7 +151,8 @@ def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, 
     """Average ms per xgpuCudaXengineDevice call (input resident in HBM)."""
     c = xg.Correlator(n, f, t, engine=engine, compute=compute, output="int32", order="tri",
                       device=torch.cuda.current_device())
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the engine launches and the timing events share it.
+    stream = torch.cuda.Stream()
     c.set_stream(stream.cuda_stream)
     nbytes = int(c.info.vecLength) * 2
     nbuf = max(1, min(max_bufs, -(-min_rotate_bytes // nbytes)))

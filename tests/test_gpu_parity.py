@@ -199,6 +199,14 @@ def test_device_input_and_offsets(xg, oracle_mod, engine):
         assert np.array_equal(got, oracle_mod.xengine_i64(x, n, f, t).astype(np.int32))
 
 
+def page_aligned(count, dtype, page=4096):
+    itemsize = np.dtype(dtype).itemsize
+    nbytes = -(-count * itemsize // page) * page
+    raw = np.zeros(nbytes + page, dtype=np.uint8)
+    start = (-raw.ctypes.data) % page
+    return raw[start: start + nbytes].view(dtype)[:count]
+
+
 def test_caller_buffers_registered_and_offsets(xg, oracle_mod):
     """Caller-allocated host buffers (registered page-rounded, or not at all)
     and input/output offsets, as xgpu.h:103-109 describes."""
@@ -210,9 +218,11 @@ def test_caller_buffers_registered_and_offsets(xg, oracle_mod):
         cfg.nstation, cfg.nfrequency, cfg.ntime, cfg.ntimepipe = n, f, t, 128
         cfg.output_type, cfg.matrix_order = xg.XGPU_INT32, xg.TRIANGULAR_ORDER
         off_in, off_out = 100, 7
-        inbuf = np.zeros(x.size + 2 * off_in + 64, dtype=np.int8)
+        # Page-aligned, page-sized buffers: registration is page-rounded, so
+        # two buffers must not share a page (as with xGPU).
+        inbuf = page_aligned(x.size + 2 * off_in + 64, np.int8)
         inbuf[2 * off_in: 2 * off_in + x.size] = x
-        outbuf = np.zeros(2 * (exact.size // 2 + off_out) + 16, dtype=np.int32)
+        outbuf = page_aligned(2 * (exact.size // 2 + off_out) + 16, np.int32)
         ctx = xg.XGPUContext()
         ctx.array_h = inbuf.ctypes.data
         ctx.array_len = inbuf.size // 2

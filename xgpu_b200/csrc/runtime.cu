@@ -173,17 +173,25 @@ int free_device(Internal *in) {
 }
 
 // Register caller memory page-rounded, as cuda_xengine.cu:386-412 does.
+// Memory the caller pinned already (cudaHostAlloc or its own registration) is
+// accepted as it is when both ends of the range are pinned; a range that
+// shares pages with other registered memory fails, as in xGPU.
 cudaError_t register_range(void *p, size_t bytes, void **registered) {
   uintptr_t a = (uintptr_t)p, base = a - (a % kPageSize);
   size_t len = bytes + (a - base);
   len = (len + kPageSize - 1) / kPageSize * kPageSize;
+  *registered = nullptr;
   cudaError_t e = cudaHostRegister((void *)base, len, cudaHostRegisterDefault);
   if (e == cudaErrorHostMemoryAlreadyRegistered) {
     cudaGetLastError();
-    *registered = nullptr;  // someone else owns the registration
-    return cudaSuccess;
+    unsigned int fl;
+    if (bytes > 0 && cudaHostGetFlags(&fl, p) == cudaSuccess &&
+        cudaHostGetFlags(&fl, (char *)p + bytes - 1) == cudaSuccess)
+      return cudaSuccess;
+    cudaGetLastError();
+    return e;
   }
-  *registered = (e == cudaSuccess) ? (void *)base : nullptr;
+  if (e == cudaSuccess) *registered = (void *)base;
   return e;
 }
 
