@@ -265,6 +265,25 @@ int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long 
  * until xgpuFree or the next xgpuSetComputeStream. */
 int xgpuSetComputeStream(XGPUContext *context, void *stream);
 
+/* Extension with no counterpart in the reference: correlate once without
+ * allocating anything, for callers that cannot call cudaMalloc where they
+ * correlate (a real-time thread that must not block on an allocation that can
+ * synchronise the device, or a plugin whose host framework owns all device
+ * memory).  cfg->ntime samples at device_input ([t][f][s][p][c] int8,
+ * 16-byte aligned) are correlated by the tensor-core engine into a fresh
+ * integration (no accumulation across calls), which is then written to
+ * device_output as cfg->matrix_order / cfg->output_type (matLength Complex).
+ * The int64 integration buffer lives in a static 32 MiB device array that
+ * every GPU loading the library holds until exit, so 64*F*N(N+1)/2 bytes must
+ * fit in 32 MiB - 256 (e.g. N=256 with F <= 15); larger sizes return
+ * XGPU_INVALID_ARGUMENT.  Work is queued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream) and the call waits for it.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised.  The
+ * first call on a device looks up the array's device address, so make it
+ * before any stream capture. */
+int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGPUConfig *cfg,
+                        int device, void *stream);
+
 /* Name of the engine a context runs ("tensor-tcgen05-int8", "plain-dp4a",
  * "plain-fp32"). */
 const char * xgpuEngineName(XGPUContext *context);

@@ -110,6 +110,9 @@ _PROTOTYPES = [
                                           ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int]),
     ("xgpuSetComputeStream", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_void_p]),
     ("xgpuEngineName", ctypes.c_char_p, [ctypes.POINTER(XGPUContext)]),
+    ("xgpuCorrelateStatic", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.POINTER(XGPUConfig), ctypes.c_int,
+                                           ctypes.c_void_p]),
 ]
 EXPORTED = [p[0] for p in _PROTOTYPES]
 
