@@ -284,6 +284,46 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream);
 int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGPUConfig *cfg,
                         int device, void *stream);
 
+/* Time splits and grid of the tensor-core engine for this context: ksplit
+ * >= 1 splits every tile's samples into that many items whose partial sums
+ * are added exactly in the integration buffer; grid is the number of CTAs
+ * (0 = one per SM).  ksplit = 0 autotunes both now: the engine is timed on
+ * synthetic input and a scratch integration buffer (the context's own is not
+ * touched) and the fastest setting is kept. */
+int xgpuTune(XGPUContext *context, int ksplit, int grid);
+
+/* ---- Extension: batches of uneven subarrays in one launch ---------------- */
+/* One subarray: its own station, channel and sample counts, its input
+ * ([t][f][s][p][c] int8, 16-byte aligned) and its int64 integration buffer
+ * (triangular order, nfrequency*nstation*(nstation+1)/2*8 values, 16-byte
+ * aligned).  accumulate = 0 replaces the buffer's contents with this run's
+ * sums; 1 adds to them.  xgpuCudaXengine's limits on sizes apply. */
+typedef struct XGPUBatchJobStruct {
+  const void *device_input;
+  long long *device_state;
+  unsigned int nstation;
+  unsigned int nfrequency;
+  unsigned int ntime;
+  int accumulate;
+} XGPUBatchJob;
+
+typedef struct XGPUBatchImpl *XGPUBatch;
+
+#define XGPU_BATCH_AUTOTUNE 1  /* time split granularity and grid chosen by timing */
+#define XGPU_BATCH_GRAPH    2  /* capture the run once as a CUDA graph and replay it */
+
+/* Plan a batch on `device`, run on `stream` (a cudaStream_t, NULL = legacy
+ * default stream).  The job list is copied; the buffers must stay valid. */
+int xgpuBatchCreate(XGPUBatch *batch, const XGPUBatchJob *jobs, int njobs, int device,
+                    void *stream, int flags);
+/* Queue one run of every job of the batch (one persistent kernel launch). */
+int xgpuBatchRun(XGPUBatch batch);
+/* Wait for queued runs; XGPU_CUDA_ERROR if a device wait timed out. */
+int xgpuBatchSync(XGPUBatch batch);
+/* Work items per run, CTAs, and samples-per-item stages chosen (0 = unsplit). */
+int xgpuBatchInfo(XGPUBatch batch, int *work_items, int *grid, int *max_steps);
+void xgpuBatchDestroy(XGPUBatch batch);
+
 /* Name of the engine a context runs ("tensor-tcgen05-int8", "plain-dp4a",
  * "plain-fp32"). */
 const char * xgpuEngineName(XGPUContext *context);

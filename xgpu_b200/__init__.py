@@ -71,6 +71,18 @@ class XGPUContext(ctypes.Structure):
     ]
 
 
+class XGPUBatchJob(ctypes.Structure):
+    """xgpu.h XGPUBatchJob (extension: one subarray of a batch)."""
+    _fields_ = [
+        ("device_input", ctypes.c_void_p), ("device_state", ctypes.c_void_p),
+        ("nstation", ctypes.c_uint), ("nfrequency", ctypes.c_uint), ("ntime", ctypes.c_uint),
+        ("accumulate", ctypes.c_int),
+    ]
+
+
+XGPU_BATCH_AUTOTUNE, XGPU_BATCH_GRAPH = 1, 2
+
+
 class XGPUConfig(ctypes.Structure):
     """xgpu.h XGPUConfig (extension: runtime sizing and engine choice)."""
     _fields_ = [
@@ -113,6 +125,15 @@ _PROTOTYPES = [
     ("xgpuCorrelateStatic", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(XGPUConfig), ctypes.c_int,
                                            ctypes.c_void_p]),
+    ("xgpuTune", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_int, ctypes.c_int]),
+    ("xgpuBatchCreate", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p),
+                                       ctypes.POINTER(XGPUBatchJob), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_int]),
+    ("xgpuBatchRun", ctypes.c_int, [ctypes.c_void_p]),
+    ("xgpuBatchSync", ctypes.c_int, [ctypes.c_void_p]),
+    ("xgpuBatchInfo", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    ("xgpuBatchDestroy", None, [ctypes.c_void_p]),
 ]
 EXPORTED = [p[0] for p in _PROTOTYPES]
 
@@ -247,6 +268,9 @@ class Correlator:
         return check("xgpuClearDeviceIntegrationBuffer",
                      lib().xgpuClearDeviceIntegrationBuffer(ctypes.byref(self.ctx)))
 
+    def tune(self, ksplit=0, grid=0):
+        return check("xgpuTune", lib().xgpuTune(ctypes.byref(self.ctx), ksplit, grid))
+
     def set_stream(self, stream_handle):
         return check("xgpuSetComputeStream",
                      lib().xgpuSetComputeStream(ctypes.byref(self.ctx),
@@ -267,6 +291,54 @@ class Correlator:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """A planned batch of uneven subarrays (xgpuBatchCreate ... xgpuBatchDestroy).
+
+    ``jobs`` is a list of dicts with keys input (device pointer), state (device
+    pointer to the int64 triangular buffer), nstation, nfrequency, ntime and
+    optionally accumulate (default 0)."""
+
+    def __init__(self, jobs, device=0, stream=None, autotune=False, graph=False):
+        arr = (XGPUBatchJob * len(jobs))()
+        for a, j in zip(arr, jobs):
+            a.device_input = j["input"]
+            a.device_state = j["state"]
+            a.nstation, a.nfrequency, a.ntime = j["nstation"], j["nfrequency"], j["ntime"]
+            a.accumulate = int(j.get("accumulate", 0))
+        self.handle = ctypes.c_void_p()
+        flags = (XGPU_BATCH_AUTOTUNE if autotune else 0) | (XGPU_BATCH_GRAPH if graph else 0)
+        check("xgpuBatchCreate", lib().xgpuBatchCreate(ctypes.byref(self.handle), arr, len(jobs),
+                                                       device, ctypes.c_void_p(stream), flags))
+
+    def run(self):
+        return check("xgpuBatchRun", lib().xgpuBatchRun(self.handle))
+
+    def sync(self):
+        return check("xgpuBatchSync", lib().xgpuBatchSync(self.handle))
+
+    def info(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check("xgpuBatchInfo", lib().xgpuBatchInfo(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                                   ctypes.byref(c)))
+        return {"work_items": a.value, "grid": b.value, "max_steps": c.value}
+
+    def close(self):
+        if self.handle:
+            lib().xgpuBatchDestroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def state_elems(nstation, nfrequency):
+    """int64 values of a triangular integration buffer."""
+    return nfrequency * nstation * (nstation + 1) // 2 * 8
 
 
 def generate_device(ptr, nbytes, kind, seed, sigma=16.0, device=0):

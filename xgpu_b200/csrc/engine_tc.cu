@@ -1,4 +1,4 @@
-// engine_tc.cu -- tcgen05 int8 tensor-core X-engine.
+// engine_tc.cu -- tcgen05 int8 tensor-core X-engine (single jobs and batches).
 //
 // The visibility matrix of one channel is the Hermitian rank-T update
 // V = sum_t x(t) x(t)^H over the 2N station-polarisation inputs
@@ -15,33 +15,49 @@
 // accumulator.  The two sums of each complex part are formed in int64 when
 // the accumulator is drained, so the result is exact.
 //
-// One CTA computes one 128x128 tile of G (32 stations x 2 pols x re/im on each
-// side) for one channel; only tiles on or below the diagonal are issued.
-//   warp 0 lane 0 : TMA producer, 3-D tiled loads with 128-byte swizzle
-//   warp 1 lane 0 : MMA issuer, tcgen05.mma.cta_group::1.kind::i8, M=N=128,
-//                   K=32 per instruction, accumulator in TMEM (128 columns)
-//   all 4 warps   : drain TMEM -> registers (tcgen05.ld 32x32b), combine the
-//                   re/im rows of each input with two warp shuffles, and add
-//                   into the int64 triangular integration buffer.
-// Every wait on an mbarrier is bounded; a timeout writes an error code and the
-// kernel still releases its TMEM and returns.
+// Work items: (job, channel, time split, 128x128 tile of G on or below the
+// diagonal), a tile being 32 stations x 2 pols x re/im on each side.  A
+// persistent grid (one CTA per SM) takes items from a static stride or from a
+// global atomic work queue (uneven batches); the producer publishes each item
+// to the other roles through a small shared-memory ring.  Six warps:
+//   warp 0    scheduler + TMA producer: 3-D tiled loads (128 bytes x 128
+//             samples, 128-byte swizzle) of row and column panels, 4 stages
+//   warp 1    TMEM owner and MMA issuer: tcgen05.mma.cta_group::1.kind::i8,
+//             M=N=128, K=32, into one of two TMEM accumulators (2 x 128
+//             columns), so a tile's drain overlaps the next tile's MMAs
+//   warps 2-5 epilogue: drain TMEM (tcgen05.ld 32x32b), combine the re/im
+//             rows of every input with two warp shuffles into int64 (re, im)
+//             pairs staged in shared memory (one 2 KB row per station), then
+//             32 lanes hand the rows to the bulk-copy engine: a plain bulk
+//             store when the item is the only writer of a zero buffer, a bulk
+//             reduce-add (cp.reduce.async.bulk .add.u64) otherwise -- the int64
+//             accumulation happens in L2 and the old values never travel to
+//             the SM, and time splits of one tile add up exactly.
+// Every mbarrier wait is bounded; a timeout writes an error code, raises a
+// CTA-wide abort flag so the other roles stop waiting, and the kernel still
+// waits (bounded) for its own copies and MMAs, frees its TMEM and returns.
 #include <cudaTypedefs.h>
 
 #include "internal.h"
+#include "tc_job.h"
 
 namespace xgpu {
 namespace tc {
 
 constexpr int kTile = 128;                 // G rows (and columns) per tile
 constexpr int kStations = kTile / 4;       // 32 stations per tile side
-constexpr int kKt = 128;                   // samples per pipeline stage
-constexpr int kStages = 3;
+constexpr int kKt = kTcSamplesPerStage;    // samples per pipeline stage
+constexpr int kStages = 4;
+constexpr int kSched = 4;                  // work-item ring between the roles
 constexpr int kBoxBytes = kTile * kKt;     // one operand of one stage: 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;
-constexpr int kBarrierBytes = 256;
-constexpr int kSmemBytes = kStages * kStageBytes + kBarrierBytes + 1024;  // + alignment slack
-constexpr uint32_t kTmemCols = 128;
-constexpr int kThreads = 128;
+constexpr int kRowPitch = kStations * 64 + 64;   // one station row of the staging tile, padded
+constexpr int kStateBytes = kStations * kRowPitch;
+constexpr int kBarrierBytes = 512;
+constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
+constexpr uint32_t kTmemCols = 2 * kTile;  // two accumulators
+constexpr int kThreads = 192;
+constexpr int kEpiThreads = 128;
 
 // Instruction descriptor (tcgen05 .kind::i8): D s32, A and B signed 8-bit,
 // both MN-major, N = 128 (bits 17-22, >>3), M = 128 (bits 24-28, >>4).
@@ -82,6 +98,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -94,13 +114,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for the phase with the given parity to complete; false after ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Wait for the phase with the given parity to complete.  Gives up (false)
+// after ~2 s, or as soon as another role raised the CTA's abort flag when
+// abort_flag is given (teardown waits pass nullptr and only time out).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          const volatile int *abort_flag) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t start = globaltimer_ns();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0 && globaltimer_ns() - start > 2000000000ull) return false;
+    if ((it & 63u) == 0) {
+      if (abort_flag && *abort_flag) return false;
+      if (globaltimer_ns() - start > 2000000000ull) return false;
+    }
   }
 }
 
@@ -111,6 +137,19 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
       " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(bar)
       : "memory");
+}
+
+__device__ __forceinline__ void bulk_store(void *dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_reduce_add(void *dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.u64 [%0], [%1], %2;" ::"l"(
+                   dst),
+               "r"(src), "r"(bytes)
+               : "memory");
 }
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
@@ -143,51 +182,127 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void epi_barrier() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
+}
+
+// Barrier over the epilogue warps that also returns whether any of their
+// threads passed v = true, so they all take the same branch afterwards.
+__device__ __forceinline__ bool epi_any(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(kEpiThreads)
+      : "memory");
+  return r != 0;
+}
+
 struct Params {
-  int n, f;
-  int t0;          // first sample of this launch
-  int nsteps;      // pipeline stages of kKt samples
-  int ntiles;      // tiles per side = ceil(4n / 128)
-  long long nbaseline;
-  int64_t *state;
-  int overwrite;
+  Job single;          // the job when jobs == nullptr (its tensor map is a parameter)
+  const Job *jobs;     // batched: job table in global memory, ordered by item_begin
+  int njobs;
+  int total;           // work items over all jobs
+  int *queue;          // dynamic work counter (zeroed before launch); nullptr: static stride
   int *err;
 };
 
-__global__ void __launch_bounds__(kThreads, 1)
-    xengine_tc_kernel(const __grid_constant__ CUtensorMap map, const Params p) {
+struct Item {
+  const Job *job;
+  int f, tr, tc;
+  int step0, nsteps;   // pipeline stages of this item (its time split)
+};
+
+__device__ __forceinline__ Item decode_item(const Params &p, int u) {
+  Item it;
+  if (p.jobs) {
+    int lo = 0, hi = p.njobs - 1;   // last job with item_begin <= u
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.jobs[mid].item_begin <= u) lo = mid; else hi = mid - 1;
+    }
+    it.job = &p.jobs[lo];
+  } else {
+    it.job = &p.single;
+  }
+  const Job &j = *it.job;
+  const int v = u - j.item_begin;
+  const int k = v % j.npairs;          // tile within the channel
+  const int rest = v / j.npairs;
+  const int split = rest % j.ksplit;
+  it.f = rest / j.ksplit;
+  int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
+  while (r * (r + 1) / 2 > k) --r;
+  while ((r + 1) * (r + 2) / 2 <= k) ++r;
+  it.tr = r;
+  it.tc = k - r * (r + 1) / 2;
+  it.step0 = split * j.steps_per_split;
+  int ns = j.total_steps - it.step0;
+  it.nsteps = ns < j.steps_per_split ? ns : j.steps_per_split;
+  return it;
+}
+
+// Bytes of station row il (0..31) of the item's tile inside the integration
+// buffer: baselines (i, j) with j in the tile's column block, j <= i, j < n.
+__device__ __forceinline__ int row_bytes(const Item &t, int il) {
+  const Job &j = *t.job;
+  const int i = t.tr * kStations + il;
+  if (i >= j.n) return 0;
+  int cnt = j.n - t.tc * kStations;
+  if (cnt > kStations) cnt = kStations;
+  if (t.tr == t.tc && il + 1 < cnt) cnt = il + 1;
+  return cnt * 64;
+}
+
+__device__ __forceinline__ int64_t *row_ptr(const Item &t, int il) {
+  const Job &j = *t.job;
+  const long long i = (long long)t.tr * kStations + il;
+  return j.state +
+         ((long long)t.f * j.nbaseline + i * (i + 1) / 2 + (long long)t.tc * kStations) * 8;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_constant__ Params p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t *bars = (uint64_t *)(smem + kStages * kStageBytes);
-  uint32_t *tmem_slot = (uint32_t *)(bars + 2 * kStages + 1);
+  uint8_t *sstate = smem + kStages * kStageBytes;
+  uint64_t *bars = (uint64_t *)(sstate + kStateBytes);
+  // full[kStages] empty[kStages] tfull[2] tempty[2] sfull[kSched] sempty[kSched] mma_done
   const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
-                 done_bar = smem_u32(bars + 2 * kStages);
+                 tfull0 = smem_u32(bars + 2 * kStages), tempty0 = smem_u32(bars + 2 * kStages + 2),
+                 sfull0 = smem_u32(bars + 2 * kStages + 4),
+                 sempty0 = smem_u32(bars + 2 * kStages + 4 + kSched),
+                 mma_done = smem_u32(bars + 2 * kStages + 4 + 2 * kSched);
+  int *sched = (int *)(bars + 2 * kStages + 5 + 2 * kSched);
+  uint32_t *tmem_slot = (uint32_t *)(sched + kSched);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // Work item: channel and lower-triangle tile (tr >= tc).
-  const int npairs = p.ntiles * (p.ntiles + 1) / 2;
-  const int f = blockIdx.x / npairs;
-  const int k = blockIdx.x - f * npairs;
-  int tr = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
-  while (tr * (tr + 1) / 2 > k) --tr;
-  while ((tr + 1) * (tr + 2) / 2 <= k) ++tr;
-  const int tcol = k - tr * (tr + 1) / 2;
-  const bool diag = (tr == tcol);
-
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
                  "r"(kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (threadIdx.x == 32) {
+  if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(done_bar, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull0 + 8 * a, 1);
+      mbar_init(tempty0 + 8 * a, kEpiThreads / 32);
+    }
+    for (int q = 0; q < kSched; ++q) {
+      mbar_init(sfull0 + 8 * q, 1);
+      mbar_init(sempty0 + 8 * q, 2);   // MMA issuer + epilogue
+    }
+    mbar_init(mma_done, 1);
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -197,93 +312,176 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
   const uint32_t stage0 = smem_u32(smem);
 
-  if (warp == 0 && lane == 0) {
-    // Producer: stage s holds the row panel at +0 and the column panel at
-    // +kBoxBytes (diagonal tiles load one panel and use it for both).
-    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&map) : "memory");
-    for (int ks = 0; ks < p.nsteps; ++ks) {
-      const int s = ks % kStages;
-      if (ks >= kStages && !mbar_wait(empty0 + 8 * s, ((ks / kStages) - 1) & 1)) {
-        atomicExch(p.err, kErrTimeoutProducer);
-        break;
-      }
-      const uint32_t dst = stage0 + s * kStageBytes;
-      mbar_expect_tx(full0 + 8 * s, diag ? kBoxBytes : 2 * kBoxBytes);
-      const int z = p.t0 + ks * kKt;
-      tma_load_3d(dst, &map, full0 + 8 * s, tr * kTile, f, z);
-      if (!diag) tma_load_3d(dst + kBoxBytes, &map, full0 + 8 * s, tcol * kTile, f, z);
-    }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer.
-    bool ok = true;
-    for (int ks = 0; ks < p.nsteps; ++ks) {
-      const int s = ks % kStages;
-      if (!mbar_wait(full0 + 8 * s, (ks / kStages) & 1)) {
-        atomicExch(p.err, kErrTimeoutMma);
-        ok = false;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a = stage0 + s * kStageBytes;
-      const uint32_t b = diag ? a : a + kBoxBytes;
-#pragma unroll
-      for (int kk = 0; kk < kKt / 32; ++kk) {
-        // 32 samples = 4 swizzle atoms = 4096 bytes per instruction.
-        mma_i8(tmem, mn_sw128_desc(a + kk * 4096), mn_sw128_desc(b + kk * 4096),
-               (ks | kk) != 0 ? 1u : 0u);
-      }
-      mma_commit(empty0 + 8 * s);
-    }
-    if (ok) mma_commit(done_bar);
-  }
-  __syncwarp();
+  auto fail = [&](int code) {
+    atomicExch(p.err, code);
+    *abort_flag = 1;
+  };
 
-  // Epilogue: warp w owns TMEM lanes (= G rows) 32w .. 32w+31.
-  const bool have = mbar_wait(done_bar, 0);
-  __syncwarp();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (!have) {
-    if (lane == 0) atomicExch(p.err, kErrTimeoutDrain);
-  } else {
-    const int m = warp * 32 + lane;
-    const int c = m & 1;               // 0: real row, 1: imaginary row
-    const int p1 = (m >> 1) & 1;
-    const int i = tr * kStations + (m >> 2);
-    const long long row_base = (long long)f * p.nbaseline + (long long)i * (i + 1) / 2;
-#pragma unroll 1
-    for (int q = 0; q < kTile / 32; ++q) {
-      uint32_t v[32];
-      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 32), v);
-#pragma unroll
-      for (int jj = 0; jj < 8; ++jj) {
-        // Columns 4jj..4jj+3 of this chunk: (p2=0 re, p2=0 im, p2=1 re, p2=1 im)
-        // of station j.  The real-row lane produces p2 = 0, the imaginary-row
-        // lane p2 = 1; each needs two values from its partner lane.
-        const int v0 = (int)v[4 * jj], v1 = (int)v[4 * jj + 1];
-        const int v2 = (int)v[4 * jj + 2], v3 = (int)v[4 * jj + 3];
-        const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
-        const int rb = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
-        const long long re = c ? (long long)ra + v3 : (long long)v0 + rb;
-        const long long im = c ? (long long)v2 - rb : (long long)ra - v1;
-        const int j = tcol * kStations + q * 8 + jj;
-        if (i < p.n && j < p.n && j <= i) {
-          longlong2 *dst = (longlong2 *)(p.state + ((row_base + j) * 4 + p1 * 2 + c) * 2);
-          if (p.overwrite) {
-            *dst = make_longlong2(re, im);
-          } else {
-            longlong2 o = *dst;
-            o.x += re;
-            o.y += im;
-            *dst = o;
+  if (warp == 0) {
+    // ------------------------------------------------ scheduler + producer --
+    if (lane == 0) {
+      if (!p.jobs) asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.single.map) : "memory");
+      uint32_t g = 0;
+      bool ok = true;
+      for (int i = 0; ok; ++i) {
+        const int slot = i % kSched;
+        if (i >= kSched && !mbar_wait(sempty0 + 8 * slot, ((i / kSched) - 1) & 1, abort_flag)) {
+          fail(kErrTimeoutProducer);
+          break;
+        }
+        const int u = p.queue ? atomicAdd(p.queue, 1) : (int)blockIdx.x + i * (int)gridDim.x;
+        ((volatile int *)sched)[slot] = u;
+        mbar_arrive(sfull0 + 8 * slot);
+        if (u >= p.total) break;
+        const Item t = decode_item(p, u);
+        const bool diag = (t.tr == t.tc);
+        const CUtensorMap *map = &t.job->map;
+        for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
+          const uint32_t s = g % kStages;
+          if (g >= (uint32_t)kStages &&
+              !mbar_wait(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort_flag)) {
+            fail(kErrTimeoutProducer);
+            ok = false;
+            break;
           }
+          const uint32_t dst = stage0 + s * kStageBytes;
+          mbar_expect_tx(full0 + 8 * s, diag ? kBoxBytes : 2 * kBoxBytes);
+          const int z = t.job->t0 + (t.step0 + ks) * kKt;
+          tma_load_3d(dst, map, full0 + 8 * s, t.tr * kTile, t.f, z);
+          if (!diag) tma_load_3d(dst + kBoxBytes, map, full0 + 8 * s, t.tc * kTile, t.f, z);
         }
       }
+      // Loads still in flight land before the CTA leaves (a no-op normally).
+      for (uint32_t q = (g > (uint32_t)kStages ? g - kStages : 0); q < g; ++q)
+        mbar_wait(full0 + 8 * (q % kStages), (q / kStages) & 1, nullptr);
     }
+  } else if (warp == 1) {
+    // --------------------------------------------------------------- MMA --
+    if (lane == 0) {
+      uint32_t g = 0;
+      bool ok = true;
+      for (int i = 0; ok; ++i) {
+        const int slot = i % kSched;
+        if (!mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)) {
+          fail(kErrTimeoutMma);
+          break;
+        }
+        const int u = ((volatile int *)sched)[slot];
+        mbar_arrive(sempty0 + 8 * slot);
+        if (u >= p.total) break;
+        const Item t = decode_item(p, u);
+        const bool diag = (t.tr == t.tc);
+        const int acc = i & 1;
+        if (i >= 2 && !mbar_wait(tempty0 + 8 * acc, ((i >> 1) - 1) & 1, abort_flag)) {
+          fail(kErrTimeoutMma);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(acc * kTile);
+        for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
+          const uint32_t s = g % kStages;
+          if (!mbar_wait(full0 + 8 * s, (g / kStages) & 1, abort_flag)) {
+            fail(kErrTimeoutMma);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a = stage0 + s * kStageBytes;
+          const uint32_t b = diag ? a : a + kBoxBytes;
+#pragma unroll
+          for (int kk = 0; kk < kKt / 32; ++kk) {
+            // 32 samples = 4 swizzle atoms = 4096 bytes per instruction.
+            mma_i8(d, mn_sw128_desc(a + kk * 4096), mn_sw128_desc(b + kk * 4096),
+                   (ks | kk) != 0 ? 1u : 0u);
+          }
+          mma_commit(empty0 + 8 * s);
+        }
+        if (ok) mma_commit(tfull0 + 8 * acc);
+      }
+      // Every MMA issued by this CTA has completed once mma_done fires.
+      mma_commit(mma_done);
+      mbar_wait(mma_done, 0, nullptr);
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue --
+    const int ew = warp - 2;                 // 0..3; warp ew == 0 issues the copies
+    const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31
+    const int m = quarter * 32 + lane;       // G row of this thread
+    const int c = m & 1;                     // 0: real row, 1: imaginary row
+    const int p1 = (m >> 1) & 1;
+    const int il = m >> 2;                   // station within the row block
+    const bool copier = (ew == 0);           // lane r copies staging row r
+    for (int i = 0;; ++i) {
+      const int slot = i % kSched;
+      const bool got = mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
+      const int u = got ? ((volatile int *)sched)[slot] : 0;
+      if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");  // staging free
+      if (epi_any(!got)) {
+        if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
+        break;
+      }
+      // every epilogue thread has read the slot
+      if (ew == 0 && lane == 0) mbar_arrive(sempty0 + 8 * slot);
+      if (u >= p.total) break;
+      const Item t = decode_item(p, u);
+      const Job &job = *t.job;
+      const int acc = i & 1;
+      const bool have = mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag);
+      if (epi_any(!have)) {
+        if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
+        break;
+      }
+      __syncwarp();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+      int jmax = job.n - t.tc * kStations;
+      if (jmax > kStations) jmax = kStations;
+      if (t.tr == t.tc && il + 1 < jmax) jmax = il + 1;
+      if (t.tr * kStations + il >= job.n) jmax = 0;
+#pragma unroll 1
+      for (int q = 0; q < kTile / 32; ++q) {
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kTile + q * 32), v);
+        if (q == kTile / 32 - 1) {
+          // Accumulator fully read: the MMA warp may reuse it.
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(tempty0 + 8 * acc);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          // Columns 4jj..4jj+3: (p2=0 re, p2=0 im, p2=1 re, p2=1 im) of station
+          // j.  The real-row lane produces p2 = 0, the imaginary-row lane p2 = 1;
+          // each needs two values from its partner lane.
+          const int v0 = (int)v[4 * jj], v1 = (int)v[4 * jj + 1];
+          const int v2 = (int)v[4 * jj + 2], v3 = (int)v[4 * jj + 3];
+          const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
+          const int rb = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
+          const long long re = c ? (long long)ra + v3 : (long long)v0 + rb;
+          const long long im = c ? (long long)v2 - rb : (long long)ra - v1;
+          const int jl = q * 8 + jj;
+          if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
+        }
+      }
+      // Staging rows complete: hand them to the bulk-copy engine.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      epi_barrier();
+      if (copier) {
+        const int nb = row_bytes(t, lane);
+        if (nb) {
+          const uint32_t src = smem_u32(sstate + lane * kRowPitch);
+          if (job.store) bulk_store(row_ptr(t, lane), src, nb);
+          else bulk_reduce_add(row_ptr(t, lane), src, nb);
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      }
+    }
+    if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTmemCols)
                  : "memory");
@@ -315,6 +513,19 @@ int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
   return r == CUDA_SUCCESS ? 0 : -3;
 }
 
+static int tc_num_sms() {
+  static int num_sms = 0;
+  if (!num_sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      num_sms = 0;
+      return 0;
+    }
+  }
+  return num_sms;
+}
+
 cudaError_t tc_check_device() {
   cudaFuncAttributes a;
   cudaError_t e = cudaFuncGetAttributes(&a, tc::xengine_tc_kernel);
@@ -323,8 +534,45 @@ cudaError_t tc_check_device() {
                               tc::kSmemBytes);
 }
 
+int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount, int64_t *state,
+                int store, int ksplit, int item_begin) {
+  if (make_tc_tensor_map(&job->map, dev_in, s) != 0) return -1;
+  const long long ntl = (4LL * s.n + tc::kTile - 1) / tc::kTile;
+  const long long npairs = ntl * (ntl + 1) / 2;
+  const int total_steps = (tcount + tc::kKt - 1) / tc::kKt;
+  if (ksplit < 1) ksplit = 1;
+  if (ksplit > total_steps) ksplit = total_steps;
+  const int per = (total_steps + ksplit - 1) / ksplit;
+  ksplit = (total_steps + per - 1) / per;   // every split non-empty
+  if ((long long)s.f * npairs * ksplit + item_begin > 0x7fffffffLL) return -2;
+  job->state = state;
+  job->nbaseline = s.nbaseline;
+  job->n = s.n;
+  job->f = s.f;
+  job->t0 = t0;
+  job->total_steps = total_steps;
+  job->steps_per_split = per;
+  job->ksplit = ksplit;
+  job->npairs = (int)npairs;
+  job->items = (int)(s.f * npairs * ksplit);
+  job->item_begin = item_begin;
+  job->store = (store && ksplit == 1) ? 1 : 0;
+  return 0;
+}
+
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                       int overwrite, int *err, cudaStream_t st) {
+  TcTuning tune;
+  tune.ksplit = 1;
+  tune.grid = 0;
+  return launch_tc_tuned(map, s, t0, tcount, state, overwrite, err, st, tune);
+}
+
+cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
+                            int64_t *state, int overwrite, int *err, cudaStream_t st,
+                            const TcTuning &tune) {
+  const int sms = tc_num_sms();
+  if (!sms) return cudaErrorInvalidDevice;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(
@@ -333,17 +581,67 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
     configured = true;
   }
   tc::Params p;
-  p.n = s.n;
-  p.f = s.f;
-  p.t0 = t0;
-  p.nsteps = (tcount + tc::kKt - 1) / tc::kKt;
-  p.ntiles = (4 * s.n + tc::kTile - 1) / tc::kTile;
-  p.nbaseline = s.nbaseline;
-  p.state = state;
-  p.overwrite = overwrite;
+  p.single.map = map;
+  // the map was encoded for `map`'s own buffer; fill the rest of the job
+  Job &j = p.single;
+  const long long ntl = (4LL * s.n + tc::kTile - 1) / tc::kTile;
+  const long long npairs = ntl * (ntl + 1) / 2;
+  const int total_steps = (tcount + tc::kKt - 1) / tc::kKt;
+  int ksplit = tune.ksplit < 1 ? 1 : (tune.ksplit > total_steps ? total_steps : tune.ksplit);
+  const int per = (total_steps + ksplit - 1) / ksplit;
+  ksplit = (total_steps + per - 1) / per;
+  if ((long long)s.f * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
+  // Split items of one tile all add into the buffer: a zero buffer must be
+  // cleared first when it would otherwise be stored into.
+  if (overwrite && ksplit > 1) {
+    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
+    if (e != cudaSuccess) return e;
+  }
+  j.state = state;
+  j.nbaseline = s.nbaseline;
+  j.n = s.n;
+  j.f = s.f;
+  j.t0 = t0;
+  j.total_steps = total_steps;
+  j.steps_per_split = per;
+  j.ksplit = ksplit;
+  j.npairs = (int)npairs;
+  j.items = (int)(s.f * npairs * ksplit);
+  j.item_begin = 0;
+  j.store = (overwrite && ksplit == 1) ? 1 : 0;
+  p.jobs = nullptr;
+  p.njobs = 1;
+  p.total = j.items;
+  p.queue = nullptr;
   p.err = err;
-  const long long grid = (long long)s.f * p.ntiles * (p.ntiles + 1) / 2;
-  tc::xengine_tc_kernel<<<(unsigned)grid, tc::kThreads, tc::kSmemBytes, st>>>(map, p);
+  int grid = tune.grid > 0 ? tune.grid : sms;
+  if (grid > p.total) grid = p.total;
+  tc::xengine_tc_kernel<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
+                            int grid, cudaStream_t st) {
+  const int sms = tc_num_sms();
+  if (!sms) return cudaErrorInvalidDevice;
+  cudaError_t e = cudaFuncSetAttribute(tc::xengine_tc_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes);
+  if (e != cudaSuccess) return e;
+  if (queue) {
+    e = cudaMemsetAsync(queue, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+  }
+  tc::Params p;
+  memset(&p.single, 0, sizeof(p.single));
+  p.jobs = dev_jobs;
+  p.njobs = njobs;
+  p.total = total_items;
+  p.queue = queue;
+  p.err = err;
+  if (grid <= 0) grid = sms;
+  if (grid > total_items) grid = total_items;
+  if (grid < 1) return cudaSuccess;
+  tc::xengine_tc_kernel<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(p);
   return cudaGetLastError();
 }
 

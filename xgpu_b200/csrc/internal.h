@@ -7,6 +7,7 @@
 #include <stdio.h>
 
 #include "../../include/xgpu.h"
+#include "tc_job.h"
 
 namespace xgpu {
 
@@ -55,6 +56,17 @@ cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcou
 // Tensor-core engine.  The tensor map describes `in` (see make_tc_tensor_map).
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                       int64_t *state, int overwrite, int *err, cudaStream_t st);
+cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
+                            int64_t *state, int overwrite, int *err, cudaStream_t st,
+                            const TcTuning &tune);
+// A batch of jobs from a device-resident table (item_begin ascending); with a
+// queue (device int) the CTAs take items dynamically, otherwise by stride.
+cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
+                            int grid, cudaStream_t st);
+// Fill a job for samples [t0, t0+tcount) of dev_in (sizes s).  store=1 asks for
+// plain stores (only honoured without time splits).  Returns 0 on success.
+int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount, int64_t *state,
+                int store, int ksplit, int item_begin);
 // Encodes the 3-D tensor map {x: 4n bytes, y: f, z: t} over a device input
 // buffer.  Returns 0 on success.
 int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);

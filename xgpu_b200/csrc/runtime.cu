@@ -75,6 +75,7 @@ struct Internal {
   cudaEvent_t comp_done[2] = {nullptr, nullptr};
   int cur = 0;
   bool state_zero = true;
+  TcTuning tune{1, 0};   // tensor-core time splits and grid
 
   // tensor maps, cached by device pointer
   struct MapEntry {
@@ -235,8 +236,8 @@ int run_engine(Internal *in, const void *d_input) {
     }
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      XGPU_CHECK(launch_tc(*map, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0, in->d_err,
-                           in->s_comp));
+      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
+                                 in->d_err, in->s_comp, in->tune));
     }
   }
   in->state_zero = false;
@@ -605,6 +606,72 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream) {
   XGPU_CHECK(cudaEventDestroy(ev));
   in->s_comp = next;
   return XGPU_OK;
+}
+
+int xgpuTune(XGPUContext *context, int ksplit, int grid) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  if (ksplit < 0 || grid < 0) return XGPU_INVALID_ARGUMENT;
+  if (ksplit > 0) {
+    in->tune.ksplit = ksplit;
+    in->tune.grid = grid;
+    return XGPU_OK;
+  }
+  if (!in->int_state || in->cfg.engine != XGPU_ENGINE_TENSOR) return XGPU_OK;  // nothing to tune
+  XGPU_CHECK(cudaSetDevice(in->device));
+  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  const Sizes &s = in->sz;
+  // Synthetic input in the first input buffer (its contents are replaced by
+  // the next xgpuCudaXengine anyway) and a scratch integration buffer.
+  XGPU_CHECK(launch_generate(in->d_in[0], (size_t)(2 * s.vec_length), 0, 12345, 16.0, in->s_comp));
+  void *scratch = nullptr;
+  if (cudaMalloc(&scratch, (size_t)s.state_elems * 8) != cudaSuccess) {
+    cudaGetLastError();
+    return XGPU_OUT_OF_MEMORY;
+  }
+  CUtensorMap map;
+  if (make_tc_tensor_map(&map, in->d_in[0], s) != 0) {
+    cudaFree(scratch);
+    return XGPU_CUDA_ERROR;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  TcTuning best_t = in->tune;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, in->device);
+  const int splits[] = {1, 2, 3, 4, 6, 8};
+  int rc = XGPU_OK;
+  for (int ks : splits) {
+    TcTuning t{ks, 0};
+    auto run = [&]() {
+      for (int t0 = 0; t0 < s.t; t0 += kSegment) {
+        const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
+        if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t) !=
+            cudaSuccess)
+          return false;
+      }
+      return true;
+    };
+    if (!run()) { rc = XGPU_CUDA_ERROR; break; }
+    cudaEventRecord(e0, in->s_comp);
+    for (int r = 0; r < 5; ++r) run();
+    cudaEventRecord(e1, in->s_comp);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = XGPU_CUDA_ERROR; break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      best_t = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  if (rc != XGPU_OK) return rc;
+  in->tune = best_t;
+  return check_device_error(in);
 }
 
 int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long long seed,

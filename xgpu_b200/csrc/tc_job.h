@@ -1,0 +1,35 @@
+// tc_job.h -- one unit of work for the tensor-core engine: an input buffer
+// (through its TMA tensor map), a sample range and an int64 integration
+// buffer.  A launch runs one job (passed as a kernel parameter) or a table of
+// jobs in device memory (uneven batches); each job is cut into work items of
+// (channel, time split, 128x128 tile).
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+namespace xgpu {
+
+constexpr int kTcSamplesPerStage = 128;
+
+struct Job {
+  CUtensorMap map;        // 3-D map {4n bytes, f, t} over the job's int8 input (64-byte aligned)
+  int64_t *state;         // triangular int64 integration buffer of the job
+  long long nbaseline;    // n(n+1)/2
+  int n, f;
+  int t0;                 // first sample of the range
+  int total_steps;        // pipeline stages (of kTcSamplesPerStage samples) in the range
+  int steps_per_split;    // stages per time split
+  int ksplit;             // time splits (each adds its partial sums into the buffer)
+  int npairs;             // lower-triangle tiles per channel
+  int items;              // f * npairs * ksplit
+  int item_begin;         // first work item of this job in the launch
+  int store;              // 1: sole writer of a zero buffer (store); 0: reduce-add
+};
+
+struct TcTuning {
+  int ksplit;             // time splits per tile (1 = none)
+  int grid;               // CTAs (0 = one per SM)
+};
+
+}  // namespace xgpu
