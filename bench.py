@@ -203,6 +203,112 @@ def e2e_ms(xg, oracle, n, f, t, steps, warmup, device):
     return ms, h2d, d2h, ok
 
 
+def config4_shapes(seed=3, k=96):
+    """96 subarrays: N log-uniform in [32,1024] rounded to 16, F uniform in
+    [1,64], T a uniform multiple of 256 in [256,8192], sigma uniform in [4,32]."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n = np.clip(np.round(np.exp(rng.uniform(np.log(32), np.log(1024), k)) / 16).astype(int) * 16,
+                32, 1024)
+    f = rng.integers(1, 65, k)
+    t = 256 * rng.integers(1, 33, k)
+    sig = rng.uniform(4, 32, k)
+    return [(int(a), int(b_), int(c), float(d)) for a, b_, c, d in zip(n, f, t, sig)]
+
+
+def bench_config4(xg, torch, steps):
+    """One persistent launch over 96 uneven subarrays (autotuned, CUDA graph)
+    vs the same jobs run one by one on the tensor-core and plain engines."""
+    shapes = config4_shapes()
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()
+    inputs, states, jobs = [], [], []
+    for q, (n, f, t, sig) in enumerate(shapes):
+        x = torch.empty(4 * n * f * t, dtype=torch.int8, device="cuda")
+        xg.generate_device(x.data_ptr(), x.numel(), 0, 3000 + q, sig, dev)
+        s = torch.empty(xg.state_elems(n, f), dtype=torch.int64, device="cuda")
+        inputs.append(x)
+        states.append(s)
+        jobs.append({"input": x.data_ptr(), "state": s.data_ptr(), "nstation": n,
+                     "nfrequency": f, "ntime": t})
+    total_ops = sum(ops(n, f, t) for n, f, t, _ in shapes)
+    out = {"jobs": len(shapes), "total_ops": total_ops}
+    with xg.Batch(jobs, device=dev, stream=stream.cuda_stream, autotune=True, graph=True) as b:
+        b.run()
+        b.sync()
+        out["tuning"] = b.info()
+        k = max(2, min(steps, 10))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            b.run()
+        e1.record(stream)
+        b.sync()
+        ms = e0.elapsed_time(e1) / k
+    out["batched_ms"] = ms
+    out["batched_tops"] = total_ops / (ms * 1e-3) / 1e12
+    batched = [s.clone() for s in states[:6]]
+    # job by job on each engine (per-call device time summed)
+    for engine in ("tensor", "plain"):
+        tot = 0.0
+        for q, (n, f, t, _) in enumerate(shapes):
+            with xg.Correlator(n, f, t, ntimepipe=256, engine=engine, device=dev) as c:
+                st = torch.cuda.Stream()
+                c.set_stream(st.cuda_stream)
+                c.run_device(inputs[q].data_ptr(), xg.SYNCOP_SYNC_COMPUTE)   # warm
+                c.clear()
+                a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a0.record(st)
+                c.run_device(inputs[q].data_ptr(), xg.SYNCOP_NONE)
+                a1.record(st)
+                a1.synchronize()
+                tot += a0.elapsed_time(a1)
+                if engine == "plain" and q < len(batched):
+                    out.setdefault("bit_exact_vs_plain", True)
+                    got = torch.from_numpy(c.dump_int64()).cuda()
+                    out["bit_exact_vs_plain"] &= bool(torch.equal(got, batched[q]))
+        out[f"{engine}_job_by_job_ms"] = tot
+        out[f"{engine}_job_by_job_tops"] = total_ops / (tot * 1e-3) / 1e12
+    out["batched_over_plain_job_by_job"] = out["plain_job_by_job_ms"] / out["batched_ms"]
+    del inputs, states
+    torch.cuda.empty_cache()
+    return out
+
+
+def config5_requests(seconds, seed=4, rate_jobs=200.0):
+    """Poisson arrivals of config-4-mix subarrays, each integrating 4-32 blocks."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate_jobs)
+        if t > seconds:
+            break
+        n = int(min(1024, max(32, round(np.exp(rng.uniform(np.log(32), np.log(1024))) / 16) * 16)))
+        reqs.append({"nstation": n, "nfrequency": int(rng.integers(1, 65)),
+                     "ntime": int(256 * rng.integers(1, 33)), "nblocks": int(rng.integers(4, 33)),
+                     "seed": 5000 + len(reqs), "sigma": float(rng.uniform(4, 32)),
+                     "arrival_s": float(t)})
+    return reqs
+
+
+SAMPLE_RATE = 1.0e5   # per-channel complex samples/s of the served stream
+
+
+def bench_config5(xg, seconds, plain_seconds, device):
+    reqs = config5_requests(seconds)
+    st, _ = xg.serve(reqs, SAMPLE_RATE, 120 << 30, host_budget_bytes=24 << 30, device=device)
+    out = {"arrival_rate_per_s": 200.0, "seconds": seconds, "sample_rate_hz": SAMPLE_RATE,
+           "requests": len(reqs), "served": st}
+    if plain_seconds > 0:
+        reqs_p = config5_requests(plain_seconds)
+        sp, _ = xg.serve(reqs_p, SAMPLE_RATE, 120 << 30, mode=xg.XGPU_SERVE_PLAIN_SERIAL,
+                         host_budget_bytes=8 << 30, device=device)
+        out["plain_serial"] = sp
+        out["plain_serial_seconds_of_arrivals"] = plain_seconds
+    return out
+
+
 def int8_peak_tops(torch):
     """Dense int8 tensor throughput of cuBLASLt (torch._int_mm) at 8192^3."""
     try:
@@ -291,7 +397,12 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-detail", action="store_true", help="skip the plain/N=512 legs")
+    ap.add_argument("--no-detail", action="store_true",
+                    help="skip the plain, N=512, batched and served legs")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="seconds of Poisson arrivals for the served stream (60 = full config)")
+    ap.add_argument("--plain-serve-seconds", type=float, default=0.5,
+                    help="seconds of arrivals for the one-at-a-time plain baseline")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
@@ -324,6 +435,13 @@ def main():
                                   sigma=40.0, min_rotate_bytes=0, max_bufs=1)
         detail["tc_n512_tops"] = ops(N3, F3, T3) / (ms3 * 1e-3) / 1e12
         detail["tc_n512_ms_per_block"] = ms3
+        if rank == 0:
+            detail["config4_batched"] = bench_config4(xg, torch, args.steps)
+            c5 = bench_config5(xg, args.serve_seconds, args.plain_serve_seconds, local)
+            detail["config5_served"] = c5
+            detail["served_p50_dump_ms"] = c5["served"]["dump_p50_ms"]
+            detail["served_p99_dump_ms"] = c5["served"]["dump_p99_ms"]
+            detail["served_tops"] = c5["served"]["tops"]
 
     e2e_v = None
     if rank == 0:

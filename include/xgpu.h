@@ -324,6 +324,58 @@ int xgpuBatchSync(XGPUBatch batch);
 int xgpuBatchInfo(XGPUBatch batch, int *work_items, int *grid, int *max_steps);
 void xgpuBatchDestroy(XGPUBatch batch);
 
+/* ---- Extension: continuous-batching server ------------------------------- */
+/* One request: a subarray integrating nblocks blocks of ntime samples per
+ * channel.  Block b's samples become available at
+ * arrival_s + (b+1) * ntime / sample_rate_hz, already in device memory as a
+ * network card would leave them: a slice of a receive pool of seeded
+ * Gaussian int8 samples filled before the clock starts (one pool per sigma
+ * bucket 4, 8, 16, 32, nearest in log2; the slice starts at byte
+ * 256 * (splitmix64(seed * 1000003 + b) mod 2^20) of the generator stream with
+ * seed 0x5EED0000 + bucket).  The request is dumped (triangular order, int32
+ * Complex) after its last block and, if dump_every > 0, after every
+ * dump_every blocks.  Requests must be sorted by arrival_s. */
+typedef struct XGPUServeJobStruct {
+  unsigned int nstation;
+  unsigned int nfrequency;
+  unsigned int ntime;        /* <= 32768 */
+  unsigned int nblocks;
+  unsigned int dump_every;
+  unsigned long long seed;
+  double sigma;
+  double arrival_s;
+} XGPUServeJob;
+
+#define XGPU_SERVE_BATCHED      0  /* continuous batching on the tensor-core engine */
+#define XGPU_SERVE_PLAIN_SERIAL 1  /* one request at a time, plain dp4a engine */
+
+typedef struct XGPUServeOptionsStruct {
+  double sample_rate_hz;            /* per-channel complex sample rate */
+  size_t device_budget_bytes;       /* HBM arena for resident state (admission limit) */
+  size_t host_budget_bytes;         /* pinned host arena for dumps (0 = 8 GiB) */
+  int mode;                         /* XGPU_SERVE_* */
+  int device;
+} XGPUServeOptions;
+
+typedef struct XGPUServeStatsStruct {
+  long long jobs, blocks, dumps;
+  double ops;                       /* 16*F*T*N(N+1) summed over blocks */
+  double wall_s;                    /* from start to the last dump in host memory */
+  double tops;                      /* ops / wall_s / 1e12 */
+  double gpu_busy_s;                /* time with device work in flight */
+  double dump_p50_ms, dump_p99_ms, dump_max_ms;  /* samples available -> dump in host memory */
+  double period_ratio_p99;          /* p99 of dump latency / the request's integration period */
+  long long late_dumps;             /* dumps slower than their request's integration period */
+  long long admitted_peak;          /* most requests resident at once */
+  double device_peak_bytes;         /* peak of the HBM arena */
+} XGPUServeStats;
+
+/* Serve the request stream in real time and return when every request has
+ * been dumped.  results, if not NULL, holds one host pointer per request
+ * (NULL to skip) receiving its final dump: triLength*2 int32 words. */
+int xgpuServeRun(const XGPUServeJob *jobs, int njobs, const XGPUServeOptions *options,
+                 XGPUServeStats *stats, int **results);
+
 /* Name of the engine a context runs ("tensor-tcgen05-int8", "plain-dp4a",
  * "plain-fp32"). */
 const char * xgpuEngineName(XGPUContext *context);

@@ -62,6 +62,8 @@ def lib():
         L.oracle_gauss_thresholds.argtypes = [ctypes.c_double, ctypes.POINTER(ctypes.c_uint32)]
         L.oracle_generate.argtypes = [c_i8p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint64,
                                       ctypes.c_double]
+        L.oracle_generate_range.argtypes = [c_i8p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint64,
+                                            ctypes.c_double, ctypes.c_uint64]
         L.oracle_unpack4.argtypes = [ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t, c_i8p]
         L.oracle_num_threads.restype = ctypes.c_int
         _lib = L
@@ -86,11 +88,33 @@ def mat_length(n, f, order):
     return int(lib().oracle_mat_length(n, f, order))
 
 
-def generate(nbytes, kind, seed, sigma=16.0):
-    """Seeded synthetic bytes; kind 0 Gaussian int8, 1 packed 4+4-bit, 2 uniform [-7,7]."""
+def generate(nbytes, kind, seed, sigma=16.0, offset=0):
+    """Seeded synthetic bytes [offset, offset+nbytes) of a stream; kind 0 Gaussian
+    int8, 1 packed 4+4-bit, 2 uniform [-7,7]."""
     out = np.empty(nbytes, dtype=np.int8)
-    lib().oracle_generate(_p(out, ctypes.c_int8), nbytes, kind, seed, sigma)
+    lib().oracle_generate_range(_p(out, ctypes.c_int8), nbytes, kind, seed, sigma, offset)
     return out
+
+
+SERVE_SIGMAS = (4.0, 8.0, 16.0, 32.0)
+
+
+def serve_block_input(nstation, nfrequency, ntime, seed, sigma, block):
+    """Input of block `block` of a served request, as xgpuServeRun defines it:
+    bytes [off, off+len) of the Gaussian stream of the sigma bucket nearest
+    (in log2) to sigma, seed 0x5EED0000 + bucket, off = 256 * (splitmix64(
+    seed * 1000003 + block) mod 2^20)."""
+    import math
+    nb = 4 * nstation * nfrequency * ntime
+    bucket = min(range(len(SERVE_SIGMAS)),
+                 key=lambda q: abs(math.log2(sigma) - math.log2(SERVE_SIGMAS[q])))
+    m = (1 << 64) - 1
+    z = (seed * 1000003 + block + 0x9E3779B97F4A7C15) & m
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    z ^= z >> 31
+    off = 256 * (z % (1 << 20))
+    return generate(nb, 0, 0x5EED0000 + bucket, SERVE_SIGMAS[bucket], off)
 
 
 def gaussian_input(n, f, t, seed, sigma=16.0):

@@ -235,28 +235,36 @@ void oracle_gauss_thresholds(double sigma, uint32_t *thr /* 254 entries */) {
   }
 }
 
-void oracle_generate(int8_t *out, size_t nbytes, int kind, uint64_t seed, double sigma) {
+/* Bytes [offset, offset + nbytes) of the stream (kind, seed, sigma). */
+void oracle_generate_range(int8_t *out, size_t nbytes, int kind, uint64_t seed, double sigma,
+                           uint64_t offset) {
   uint32_t thr[254];
   if (kind == 0) oracle_gauss_thresholds(sigma, thr);
 #pragma omp parallel for schedule(static)
-  for (long n = 0; n < (long)nbytes; n++) {
-    uint32_t u = hash32(seed, (uint64_t)n);
+  for (long q = 0; q < (long)nbytes; q++) {
+    const uint64_t n = offset + (uint64_t)q;
+    int8_t *o = out + q;
+    uint32_t u = hash32(seed, n);
     if (kind == 0) {
       int lo = 0, hi = 254; /* first index with u < thr[idx], 254 if none */
       while (lo < hi) {
         int mid = (lo + hi) >> 1;
         if (u < thr[mid]) hi = mid; else lo = mid + 1;
       }
-      out[n] = (int8_t)(lo - 127);
+      *o = (int8_t)(lo - 127);
     } else if (kind == 1) {
-      uint32_t v = hash32(seed ^ 0x5A5A5A5A5A5A5A5Aull, (uint64_t)n);
+      uint32_t v = hash32(seed ^ 0x5A5A5A5A5A5A5A5Aull, n);
       int re = (int)(((uint64_t)u * 15u) >> 32) - 7;
       int im = (int)(((uint64_t)v * 15u) >> 32) - 7;
-      out[n] = (int8_t)(((re & 0xF) << 4) | (im & 0xF));
+      *o = (int8_t)(((re & 0xF) << 4) | (im & 0xF));
     } else {
-      out[n] = (int8_t)((int)(((uint64_t)u * 15u) >> 32) - 7);
+      *o = (int8_t)((int)(((uint64_t)u * 15u) >> 32) - 7);
     }
   }
+}
+
+void oracle_generate(int8_t *out, size_t nbytes, int kind, uint64_t seed, double sigma) {
+  oracle_generate_range(out, nbytes, kind, seed, sigma, 0);
 }
 
 /* Packed 4+4-bit -> int8 re/im pairs (re = high nibble, im = low nibble). */

@@ -81,6 +81,33 @@ class XGPUBatchJob(ctypes.Structure):
 
 
 XGPU_BATCH_AUTOTUNE, XGPU_BATCH_GRAPH = 1, 2
+XGPU_SERVE_BATCHED, XGPU_SERVE_PLAIN_SERIAL = 0, 1
+
+
+class XGPUServeJob(ctypes.Structure):
+    _fields_ = [
+        ("nstation", ctypes.c_uint), ("nfrequency", ctypes.c_uint), ("ntime", ctypes.c_uint),
+        ("nblocks", ctypes.c_uint), ("dump_every", ctypes.c_uint), ("seed", ctypes.c_ulonglong),
+        ("sigma", ctypes.c_double), ("arrival_s", ctypes.c_double),
+    ]
+
+
+class XGPUServeOptions(ctypes.Structure):
+    _fields_ = [
+        ("sample_rate_hz", ctypes.c_double), ("device_budget_bytes", ctypes.c_size_t),
+        ("host_budget_bytes", ctypes.c_size_t), ("mode", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class XGPUServeStats(ctypes.Structure):
+    _fields_ = [
+        ("jobs", ctypes.c_longlong), ("blocks", ctypes.c_longlong), ("dumps", ctypes.c_longlong),
+        ("ops", ctypes.c_double), ("wall_s", ctypes.c_double), ("tops", ctypes.c_double),
+        ("gpu_busy_s", ctypes.c_double), ("dump_p50_ms", ctypes.c_double),
+        ("dump_p99_ms", ctypes.c_double), ("dump_max_ms", ctypes.c_double),
+        ("period_ratio_p99", ctypes.c_double), ("late_dumps", ctypes.c_longlong),
+        ("admitted_peak", ctypes.c_longlong), ("device_peak_bytes", ctypes.c_double),
+    ]
 
 
 class XGPUConfig(ctypes.Structure):
@@ -134,6 +161,10 @@ _PROTOTYPES = [
     ("xgpuBatchInfo", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("xgpuBatchDestroy", None, [ctypes.c_void_p]),
+    ("xgpuServeRun", ctypes.c_int, [ctypes.POINTER(XGPUServeJob), ctypes.c_int,
+                                    ctypes.POINTER(XGPUServeOptions),
+                                    ctypes.POINTER(XGPUServeStats),
+                                    ctypes.POINTER(ctypes.POINTER(ctypes.c_int))]),
 ]
 EXPORTED = [p[0] for p in _PROTOTYPES]
 
@@ -334,6 +365,31 @@ class Batch:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def serve(requests, sample_rate_hz, device_budget_bytes, mode=XGPU_SERVE_BATCHED, device=0,
+          host_budget_bytes=0, collect=False):
+    """Run xgpuServeRun on a list of request dicts (nstation, nfrequency, ntime,
+    nblocks, dump_every, seed, sigma, arrival_s).  Returns (stats dict, results)
+    where results are the final int32 triangular dumps when collect=True."""
+    arr = (XGPUServeJob * len(requests))()
+    for a, r in zip(arr, requests):
+        a.nstation, a.nfrequency, a.ntime = r["nstation"], r["nfrequency"], r["ntime"]
+        a.nblocks, a.dump_every = r["nblocks"], r.get("dump_every", 0)
+        a.seed, a.sigma, a.arrival_s = r["seed"], r.get("sigma", 16.0), r["arrival_s"]
+    opt = XGPUServeOptions(sample_rate_hz, device_budget_bytes, host_budget_bytes, mode, device)
+    st = XGPUServeStats()
+    res_ptrs = None
+    results = None
+    if collect:
+        results = [np.zeros(r["nfrequency"] * r["nstation"] * (r["nstation"] + 1) // 2 * 8,
+                            dtype=np.int32) for r in requests]
+        res_ptrs = (ctypes.POINTER(ctypes.c_int) * len(requests))(
+            *[x.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) for x in results])
+    check("xgpuServeRun", lib().xgpuServeRun(arr, len(requests), ctypes.byref(opt),
+                                             ctypes.byref(st), res_ptrs))
+    stats = {name: getattr(st, name) for name, _ in XGPUServeStats._fields_}
+    return stats, results
 
 
 def state_elems(nstation, nfrequency):
