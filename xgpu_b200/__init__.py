@@ -392,6 +392,28 @@ def serve(requests, sample_rate_hz, device_budget_bytes, mode=XGPU_SERVE_BATCHED
     return stats, results
 
 
+def channel_shard(nfrequency, world, rank):
+    """Channels [f0, f1) of one GPU when nfrequency channels are split over
+    `world` GPUs (one context per GPU, no collective: channels are
+    independent).  The first nfrequency % world GPUs take one extra channel."""
+    base, extra = divmod(nfrequency, world)
+    f0 = rank * base + min(rank, extra)
+    return f0, f0 + base + (1 if rank < extra else 0)
+
+
+def shard_input(x, nstation, nfrequency, ntime, f0, f1):
+    """The [t][f][s][p][c] samples of channels [f0, f1), contiguous."""
+    a = np.asarray(x).reshape(ntime, nfrequency, nstation * 4)
+    return np.ascontiguousarray(a[:, f0:f1, :]).reshape(-1)
+
+
+def merge_triangular(parts):
+    """Full triangular-order output from per-GPU outputs of consecutive channel
+    ranges: triangular order is channel-major ([f][baseline][p1][p2][re,im]), so
+    the shards concatenate."""
+    return np.concatenate([np.asarray(q).reshape(-1) for q in parts])
+
+
 def state_elems(nstation, nfrequency):
     """int64 values of a triangular integration buffer."""
     return nfrequency * nstation * (nstation + 1) // 2 * 8

@@ -53,7 +53,7 @@ constexpr int kBoxBytes = kTile * kKt;     // one operand of one stage: 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;
 constexpr int kRowPitch = kStations * 64 + 64;   // one station row of the staging tile, padded
 constexpr int kStateBytes = kStations * kRowPitch;
-constexpr int kBarrierBytes = 512;
+constexpr int kBarrierBytes = 1024;
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
 constexpr uint32_t kTmemCols = 2 * kTile;  // two accumulators
 constexpr int kThreads = 192;
@@ -210,25 +210,34 @@ struct Params {
   int *err;
 };
 
+// A decoded work item.  The scheduler decodes each item once and publishes it
+// in a shared-memory ring; the MMA issuer and the epilogue copy it to
+// registers, so neither reads the job table on its critical path.
 struct Item {
-  const Job *job;
+  int u;               // work item index (>= total: no more work)
   int f, tr, tc;
   int step0, nsteps;   // pipeline stages of this item (its time split)
+  int n, store, t0, pad;
+  long long nbaseline;
+  int64_t *state;
+  const CUtensorMap *map;
 };
 
 __device__ __forceinline__ Item decode_item(const Params &p, int u) {
   Item it;
+  it.u = u;
+  const Job *jp;
   if (p.jobs) {
     int lo = 0, hi = p.njobs - 1;   // last job with item_begin <= u
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (p.jobs[mid].item_begin <= u) lo = mid; else hi = mid - 1;
     }
-    it.job = &p.jobs[lo];
+    jp = &p.jobs[lo];
   } else {
-    it.job = &p.single;
+    jp = &p.single;
   }
-  const Job &j = *it.job;
+  const Job &j = *jp;
   const int v = u - j.item_begin;
   const int k = v % j.npairs;          // tile within the channel
   const int rest = v / j.npairs;
@@ -240,28 +249,32 @@ __device__ __forceinline__ Item decode_item(const Params &p, int u) {
   it.tr = r;
   it.tc = k - r * (r + 1) / 2;
   it.step0 = split * j.steps_per_split;
-  int ns = j.total_steps - it.step0;
+  const int ns = j.total_steps - it.step0;
   it.nsteps = ns < j.steps_per_split ? ns : j.steps_per_split;
+  it.n = j.n;
+  it.store = j.store;
+  it.t0 = j.t0;
+  it.pad = 0;
+  it.nbaseline = j.nbaseline;
+  it.state = j.state;
+  it.map = &j.map;
   return it;
 }
 
 // Bytes of station row il (0..31) of the item's tile inside the integration
 // buffer: baselines (i, j) with j in the tile's column block, j <= i, j < n.
 __device__ __forceinline__ int row_bytes(const Item &t, int il) {
-  const Job &j = *t.job;
   const int i = t.tr * kStations + il;
-  if (i >= j.n) return 0;
-  int cnt = j.n - t.tc * kStations;
+  if (i >= t.n) return 0;
+  int cnt = t.n - t.tc * kStations;
   if (cnt > kStations) cnt = kStations;
   if (t.tr == t.tc && il + 1 < cnt) cnt = il + 1;
   return cnt * 64;
 }
 
 __device__ __forceinline__ int64_t *row_ptr(const Item &t, int il) {
-  const Job &j = *t.job;
   const long long i = (long long)t.tr * kStations + il;
-  return j.state +
-         ((long long)t.f * j.nbaseline + i * (i + 1) / 2 + (long long)t.tc * kStations) * 8;
+  return t.state + ((long long)t.f * t.nbaseline + i * (i + 1) / 2 + (long long)t.tc * kStations) * 8;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_constant__ Params p) {
@@ -275,8 +288,8 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
                  sfull0 = smem_u32(bars + 2 * kStages + 4),
                  sempty0 = smem_u32(bars + 2 * kStages + 4 + kSched),
                  mma_done = smem_u32(bars + 2 * kStages + 4 + 2 * kSched);
-  int *sched = (int *)(bars + 2 * kStages + 5 + 2 * kSched);
-  uint32_t *tmem_slot = (uint32_t *)(sched + kSched);
+  Item *ring = (Item *)(bars + 2 * kStages + 6 + 2 * kSched);   // 8-byte aligned
+  uint32_t *tmem_slot = (uint32_t *)(ring + kSched);
   volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -330,12 +343,17 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
           break;
         }
         const int u = p.queue ? atomicAdd(p.queue, 1) : (int)blockIdx.x + i * (int)gridDim.x;
-        ((volatile int *)sched)[slot] = u;
-        mbar_arrive(sfull0 + 8 * slot);
+        Item t;
+        if (u < p.total) {
+          t = decode_item(p, u);
+        } else {
+          t.u = u;
+        }
+        ring[slot] = t;
+        mbar_arrive(sfull0 + 8 * slot);   // release: the entry is visible to the waiters
         if (u >= p.total) break;
-        const Item t = decode_item(p, u);
         const bool diag = (t.tr == t.tc);
-        const CUtensorMap *map = &t.job->map;
+        const CUtensorMap *map = t.map;
         for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
           const uint32_t s = g % kStages;
           if (g >= (uint32_t)kStages &&
@@ -346,7 +364,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
           }
           const uint32_t dst = stage0 + s * kStageBytes;
           mbar_expect_tx(full0 + 8 * s, diag ? kBoxBytes : 2 * kBoxBytes);
-          const int z = t.job->t0 + (t.step0 + ks) * kKt;
+          const int z = t.t0 + (t.step0 + ks) * kKt;
           tma_load_3d(dst, map, full0 + 8 * s, t.tr * kTile, t.f, z);
           if (!diag) tma_load_3d(dst + kBoxBytes, map, full0 + 8 * s, t.tc * kTile, t.f, z);
         }
@@ -366,10 +384,9 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
           fail(kErrTimeoutMma);
           break;
         }
-        const int u = ((volatile int *)sched)[slot];
+        const Item t = ring[slot];
         mbar_arrive(sempty0 + 8 * slot);
-        if (u >= p.total) break;
-        const Item t = decode_item(p, u);
+        if (t.u >= p.total) break;
         const bool diag = (t.tr == t.tc);
         const int acc = i & 1;
         if (i >= 2 && !mbar_wait(tempty0 + 8 * acc, ((i >> 1) - 1) & 1, abort_flag)) {
@@ -414,17 +431,16 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
     for (int i = 0;; ++i) {
       const int slot = i % kSched;
       const bool got = mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
-      const int u = got ? ((volatile int *)sched)[slot] : 0;
+      Item t;
+      if (got) t = ring[slot];
       if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");  // staging free
       if (epi_any(!got)) {
         if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
         break;
       }
-      // every epilogue thread has read the slot
+      // every epilogue thread has copied the entry
       if (ew == 0 && lane == 0) mbar_arrive(sempty0 + 8 * slot);
-      if (u >= p.total) break;
-      const Item t = decode_item(p, u);
-      const Job &job = *t.job;
+      if (t.u >= p.total) break;
       const int acc = i & 1;
       const bool have = mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag);
       if (epi_any(!have)) {
@@ -434,10 +450,10 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       __syncwarp();
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
-      int jmax = job.n - t.tc * kStations;
+      int jmax = t.n - t.tc * kStations;
       if (jmax > kStations) jmax = kStations;
       if (t.tr == t.tc && il + 1 < jmax) jmax = il + 1;
-      if (t.tr * kStations + il >= job.n) jmax = 0;
+      if (t.tr * kStations + il >= t.n) jmax = 0;
 #pragma unroll 1
       for (int q = 0; q < kTile / 32; ++q) {
         uint32_t v[32];
@@ -470,7 +486,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
         const int nb = row_bytes(t, lane);
         if (nb) {
           const uint32_t src = smem_u32(sstate + lane * kRowPitch);
-          if (job.store) bulk_store(row_ptr(t, lane), src, nb);
+          if (t.store) bulk_store(row_ptr(t, lane), src, nb);
           else bulk_reduce_add(row_ptr(t, lane), src, nb);
         }
         asm volatile("cp.async.bulk.commit_group;" ::: "memory");

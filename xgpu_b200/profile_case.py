@@ -1,0 +1,65 @@
+"""Time one engine on one shape with the input resident in device memory.
+
+    python -m xgpu_b200.profile_case --n 512 --f 32 --t 8192 [--engine tensor|plain|fp32]
+                                     [--reps 5] [--warmup 3] [--ksplit K] [--accumulate]
+
+Prints one JSON line: milliseconds per xgpuCudaXengineDevice call (CUDA
+events on the engine's stream) and X-engine TOPS (16*F*T*N(N+1) ops per
+call).  Useful to size a deployment and as a small, self-contained case for
+profilers.
+"""
+import argparse
+import json
+
+import xgpu_b200 as xg
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--f", type=int, default=32)
+    ap.add_argument("--t", type=int, default=8192)
+    ap.add_argument("--engine", default="tensor", choices=["tensor", "plain", "fp32"])
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--ksplit", type=int, default=-1, help="-1: engine default, 0: autotune")
+    ap.add_argument("--accumulate", action="store_true",
+                    help="add into the integration (default: every call starts a new one)")
+    ap.add_argument("--sigma", type=float, default=16.0)
+    args = ap.parse_args()
+
+    import torch
+    compute = "fp32" if args.engine == "fp32" else "int8"
+    engine = "plain" if args.engine in ("plain", "fp32") else "tensor"
+    c = xg.Correlator(args.n, args.f, args.t, ntimepipe=16, engine=engine, compute=compute,
+                      output="int32" if compute == "int8" else "float32", order="tri")
+    if args.ksplit >= 0:
+        c.tune(args.ksplit, 0)
+    stream = torch.cuda.Stream()
+    c.set_stream(stream.cuda_stream)
+    nbytes = int(c.info.vecLength) * 2
+    x = torch.empty(nbytes, dtype=torch.int8, device="cuda")
+    xg.generate_device(x.data_ptr(), nbytes, 0, 7, args.sigma, torch.cuda.current_device())
+    for _ in range(args.warmup):
+        if not args.accumulate:
+            c.clear()
+        c.run_device(x.data_ptr(), xg.SYNCOP_NONE)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.reps):
+        if not args.accumulate:
+            c.clear()
+        c.run_device(x.data_ptr(), xg.SYNCOP_NONE)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    ops = xg.ops_per_integration(args.n, args.f, args.t)
+    print(json.dumps({"engine": c.engine_name, "n": args.n, "f": args.f, "t": args.t,
+                      "ms": ms, "tops": ops / (ms * 1e-3) / 1e12,
+                      "accumulate": args.accumulate}))
+    c.close()
+
+
+if __name__ == "__main__":
+    main()
