@@ -153,7 +153,7 @@ def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, 
     c = xg.Correlator(n, f, t, engine=engine, compute=compute, output="int32", order="tri",
                       device=torch.cuda.current_device())
     if engine == "tensor":
-        c.tune(0)
+        c.tune(0)   # kernel, time splits and grid chosen by timing
     # A dedicated stream: the engine launches and the timing events share it.
     stream = torch.cuda.Stream()
     c.set_stream(stream.cuda_stream)

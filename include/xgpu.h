@@ -284,13 +284,15 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream);
 int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGPUConfig *cfg,
                         int device, void *stream);
 
-/* Time splits and grid of the tensor-core engine for this context: ksplit
- * >= 1 splits every tile's samples into that many items whose partial sums
- * are added exactly in the integration buffer; grid is the number of CTAs
- * (0 = one per SM).  ksplit = 0 autotunes both now: the engine is timed on
- * synthetic input and a scratch integration buffer (the context's own is not
- * touched) and the fastest setting is kept. */
-int xgpuTune(XGPUContext *context, int ksplit, int grid);
+/* Kernel, time splits and grid of the tensor-core engine for this context.
+ * pair = 0 runs one CTA per 128x128 tile of the Gram matrix; pair = 1 runs
+ * CTA pairs (tcgen05 cta_group::2) on 256x256 tiles.  ksplit >= 1 splits
+ * every tile's samples into that many items whose partial sums are added
+ * exactly in the integration buffer; grid is the number of CTAs (0 = one per
+ * SM).  ksplit = 0 autotunes all three now: the engine is timed on synthetic
+ * input and a scratch integration buffer (the context's own is not touched)
+ * and the fastest setting is kept. */
+int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);
 
 /* ---- Extension: batches of uneven subarrays in one launch ---------------- */
 /* One subarray: its own station, channel and sample counts, its input

@@ -17,12 +17,13 @@ def plain_job_by_job(xg, x_dev, n, f, t):
         return c.dump_int64()
 
 
+@pytest.mark.parametrize("pair", [0, 1])
 @pytest.mark.parametrize("ksplit", [2, 3, 8])
-def test_time_splits_are_exact(xg, oracle_mod, ksplit):
+def test_time_splits_are_exact(xg, oracle_mod, ksplit, pair):
     n, f, t = 64, 3, 1024 + 384
     x = oracle_mod.gaussian_input(n, f, t, seed=ksplit, sigma=30.0)
     with xg.Correlator(n, f, t, ntimepipe=128, engine="tensor") as c:
-        c.tune(ksplit, 0)
+        c.tune(ksplit, 0, pair)
         c.set_input(x)
         c.run(xg.SYNCOP_SYNC_COMPUTE)        # first call after init stores (buffer zero)
         c.set_input(x)
@@ -42,6 +43,41 @@ def test_context_autotune_keeps_results(xg, oracle_mod):
         c.run(xg.SYNCOP_DUMP)
         got = c.dump_int64()
     assert np.array_equal(got, 2 * oracle_mod.xengine_i64(x, n, f, t))
+
+
+@pytest.mark.parametrize("n,f,t", [(16, 2, 64), (32, 3, 256), (48, 2, 128), (64, 5, 1024),
+                                   (80, 1, 512), (112, 2, 384), (128, 4, 2048), (256, 10, 1024),
+                                   (320, 2, 768), (512, 3, 8192)])
+def test_pair_kernel_parity(xg, oracle_mod, n, f, t):
+    """CTA-pair kernel (256x256 tiles): bit-exact, store and accumulate paths."""
+    x = oracle_mod.gaussian_input(n, f, t, seed=n * 7 + t, sigma=24.0)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor") as c:
+        c.tune(1, 0, 1)
+        c.set_input(x)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)    # stores into the cleared buffer
+        assert np.array_equal(c.dump_int64(), exact)
+        c.set_input(x)
+        c.run(xg.SYNCOP_DUMP)            # adds (bulk reduce-add)
+        assert np.array_equal(c.dump_int64(), 2 * exact)
+        got = c.output_view()[: c.info.matLength * 2]
+        assert np.array_equal(got, (2 * exact).astype(np.int32))
+
+
+def test_pair_kernel_small_grid_and_autotune(xg, oracle_mod):
+    n, f, t = 256, 6, 2048
+    x = oracle_mod.gaussian_input(n, f, t, seed=77)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    with xg.Correlator(n, f, t, engine="tensor") as c:
+        c.tune(3, 10, 1)                  # 5 clusters walk all items
+        c.set_input(x)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)
+        assert np.array_equal(c.dump_int64(), exact)
+        c.tune(0)                         # autotune over both kernels
+        c.clear()
+        c.set_input(x)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)
+        assert np.array_equal(c.dump_int64(), exact)
 
 
 def make_jobs(torch, oracle_mod, shapes, seed0=100):

@@ -152,7 +152,8 @@ _PROTOTYPES = [
     ("xgpuCorrelateStatic", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(XGPUConfig), ctypes.c_int,
                                            ctypes.c_void_p]),
-    ("xgpuTune", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_int, ctypes.c_int]),
+    ("xgpuTune", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int]),
     ("xgpuBatchCreate", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p),
                                        ctypes.POINTER(XGPUBatchJob), ctypes.c_int, ctypes.c_int,
                                        ctypes.c_void_p, ctypes.c_int]),
@@ -299,8 +300,10 @@ class Correlator:
         return check("xgpuClearDeviceIntegrationBuffer",
                      lib().xgpuClearDeviceIntegrationBuffer(ctypes.byref(self.ctx)))
 
-    def tune(self, ksplit=0, grid=0):
-        return check("xgpuTune", lib().xgpuTune(ctypes.byref(self.ctx), ksplit, grid))
+    def tune(self, ksplit=0, grid=0, pair=0):
+        """Tensor-core kernel choice: ksplit=0 autotunes; else fixed time splits,
+        grid (0 = one CTA per SM) and kernel (pair=1: CTA pairs, 256x256 tiles)."""
+        return check("xgpuTune", lib().xgpuTune(ctypes.byref(self.ctx), ksplit, grid, pair))
 
     def set_stream(self, stream_handle):
         return check("xgpuSetComputeStream",

@@ -1,0 +1,431 @@
+// engine_tc2.cu -- tcgen05 int8 X-engine on CTA pairs (cta_group::2), 256x256
+// tiles of the Gram matrix.
+//
+// Same arithmetic as engine_tc.cu (G = A A^T over the int8 input bytes of
+// each sample, MN-major operands straight from HBM, re/im combined in int64
+// when draining), with the tile doubled in both directions and shared by the
+// two SMs of a cluster:
+//   * the pair computes rows [256R, 256R+256) x columns [256C, 256C+256) of G
+//     (64 x 64 stations) for one channel, R >= C;
+//   * CTA r loads its own 128 rows of A (32 stations) and half r of the 256
+//     columns of B into its shared memory; the leader CTA issues
+//     tcgen05.mma.cta_group::2.kind::i8 with M = N = 256, which reads both
+//     CTAs' halves, and each CTA's TMEM receives its 128 rows x 256 columns;
+//   * per CTA and per 128 samples that is 32 KiB of loads for 128x256 output
+//     columns -- half the bytes per MMA operation of the single-CTA kernel, so
+//     the load pipeline's latency is covered with the same shared memory.
+// Cross-CTA signalling uses no multicast: TMA loads of both CTAs complete on
+// the leader's "full" barrier (.cta_group::2 form, the peer's copy names the
+// leader's barrier; only the leader registers the expected bytes, so the
+// producers issue no cross-CTA fence), the leader's MMA commits once to each CTA's "empty" and
+// "accumulator full" barriers, and the peer's epilogue arrives remotely on the
+// leader's "accumulator empty" barrier.  Every wait is bounded (as in
+// engine_tc.cu); both CTAs meet at a cluster barrier before releasing TMEM.
+#include <cudaTypedefs.h>
+
+#include "internal.h"
+#include "tc_common.cuh"
+#include "tc_job.h"
+
+namespace xgpu {
+namespace tc2 {
+
+using namespace tc;
+
+constexpr int kHalf = 128;                  // G rows per CTA; B columns per CTA
+constexpr int kStations = kHalf / 4;        // 32 stations
+constexpr int kKt = kTcSamplesPerStage;     // samples per pipeline stage
+constexpr int kStages = 4;
+constexpr int kSched = 4;
+constexpr int kBoxBytes = kHalf * kKt;      // 16 KiB
+constexpr int kStageBytes = 2 * kBoxBytes;  // A rows + B half
+constexpr int kRowPitch = kStations * 64 + 64;
+constexpr int kStateBytes = kStations * kRowPitch;   // one 32x32-station block
+constexpr int kBarrierBytes = 1024;
+constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
+constexpr uint32_t kAccCols = 2 * kHalf;    // 256 columns per accumulator
+constexpr uint32_t kTmemCols = 2 * kAccCols;
+constexpr int kThreads = 192;
+constexpr uint32_t kIdesc = i8_idesc(2 * kHalf, 2 * kHalf);
+
+struct Params {
+  Job job;     // npairs counts 256x256 tiles on or below the diagonal
+  int total;   // f * npairs * ksplit work items
+  int *err;
+};
+
+struct Item {
+  int u;
+  int f, R, C;
+  int step0, nsteps;
+};
+
+__device__ __forceinline__ Item decode(const Job &j, int u) {
+  Item it;
+  it.u = u;
+  const int k = u % j.npairs;
+  const int rest = u / j.npairs;
+  const int split = rest % j.ksplit;
+  it.f = rest / j.ksplit;
+  int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
+  while (r * (r + 1) / 2 > k) --r;
+  while ((r + 1) * (r + 2) / 2 <= k) ++r;
+  it.R = r;
+  it.C = k - r * (r + 1) / 2;
+  it.step0 = split * j.steps_per_split;
+  const int ns = j.total_steps - it.step0;
+  it.nsteps = ns < j.steps_per_split ? ns : j.steps_per_split;
+  return it;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t peer_addr(uint32_t local, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+
+// Arrive on a barrier of either CTA of the pair (default semantics: no
+// cluster-scope fence on the arriving thread).
+__device__ __forceinline__ void remote_arrive(uint32_t cluster_bar) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap *map,
+                                                 uint32_t cluster_bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(cluster_bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void commit_pair(uint32_t cluster_bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   cluster_bar)
+               : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    xengine_tc2_kernel(const __grid_constant__ Params p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *sstate = smem + kStages * kStageBytes;
+  uint64_t *bars = (uint64_t *)(sstate + kStateBytes);
+  // full[kStages] empty[kStages] tfull[2] tempty[2] sfull[kSched] sempty[kSched] mma_done
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
+                 tfull0 = smem_u32(bars + 2 * kStages), tempty0 = smem_u32(bars + 2 * kStages + 2),
+                 sfull0 = smem_u32(bars + 2 * kStages + 4),
+                 sempty0 = smem_u32(bars + 2 * kStages + 4 + kSched),
+                 mma_done = smem_u32(bars + 2 * kStages + 4 + 2 * kSched);
+  Item *ring = (Item *)(bars + 2 * kStages + 6 + 2 * kSched);
+  uint32_t *tmem_slot = (uint32_t *)(ring + kSched);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = (rank == 0);
+  const int cid = (int)(blockIdx.x >> 1), ncl = (int)(gridDim.x >> 1);
+  const Job &job = p.job;
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);     // the leader's arrival; both CTAs' loads complete on it
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull0 + 8 * a, 1);
+      mbar_init(tempty0 + 8 * a, 2 * kEpiThreads / 32);   // epilogue warps of both CTAs
+    }
+    for (int q = 0; q < kSched; ++q) {
+      mbar_init(sfull0 + 8 * q, 1);
+      mbar_init(sempty0 + 8 * q, 2);
+    }
+    mbar_init(mma_done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cluster_sync();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t stage0 = smem_u32(smem);
+
+  auto fail = [&](int code) {
+    atomicExch(p.err, code);
+    *abort_flag = 1;
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------ scheduler + producer --
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&job.map) : "memory");
+      uint32_t g = 0;
+      bool ok = true;
+      for (int i = 0; ok; ++i) {
+        const int slot = i % kSched;
+        if (i >= kSched && !mbar_wait(sempty0 + 8 * slot, ((i / kSched) - 1) & 1, abort_flag)) {
+          fail(kErrTimeoutProducer);
+          break;
+        }
+        const int u = cid + i * ncl;
+        Item t;
+        if (u < p.total) t = decode(job, u); else t.u = u;
+        ring[slot] = t;
+        mbar_arrive(sfull0 + 8 * slot);
+        if (u >= p.total) break;
+        const bool diag = (t.R == t.C);
+        const int rb = 2 * t.R + (int)rank, cbb = 2 * t.C + (int)rank;
+        for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
+          const uint32_t s = g % kStages;
+          if (g >= (uint32_t)kStages &&
+              !mbar_wait(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort_flag)) {
+            fail(kErrTimeoutProducer);
+            ok = false;
+            break;
+          }
+          const uint32_t dst = stage0 + s * kStageBytes;
+          const uint32_t fbar = peer_addr(full0 + 8 * s, 0);
+          // The leader expects the bytes of both CTAs; the peer's loads may land
+          // first (the transaction count then dips below zero until it does).
+          if (leader) mbar_expect_tx(full0 + 8 * s, diag ? 2 * kBoxBytes : 4 * kBoxBytes);
+          const int z = job.t0 + (t.step0 + ks) * kKt;
+          tma_load_3d_pair(dst, &job.map, fbar, rb * kHalf, t.f, z);
+          if (!diag) tma_load_3d_pair(dst + kBoxBytes, &job.map, fbar, cbb * kHalf, t.f, z);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // --------------------------------------------------------------- MMA --
+    if (lane == 0) {
+      uint32_t g = 0;
+      bool ok = true;
+      bool issued = false;
+      for (int i = 0; ok; ++i) {
+        const int slot = i % kSched;
+        if (!mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)) {
+          fail(kErrTimeoutMma);
+          break;
+        }
+        const Item t = ring[slot];
+        mbar_arrive(sempty0 + 8 * slot);
+        if (t.u >= p.total) break;
+        if (!leader) continue;   // the leader issues the pair's MMAs
+        const bool diag = (t.R == t.C);
+        const int acc = i & 1;
+        if (i >= 2 && !mbar_wait(tempty0 + 8 * acc, ((i >> 1) - 1) & 1, abort_flag)) {
+          fail(kErrTimeoutMma);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(acc * kAccCols);
+        for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
+          const uint32_t s = g % kStages;
+          if (!mbar_wait(full0 + 8 * s, (g / kStages) & 1, abort_flag)) {
+            fail(kErrTimeoutMma);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a = stage0 + s * kStageBytes;
+          const uint32_t b = diag ? a : a + kBoxBytes;
+#pragma unroll
+          for (int kk = 0; kk < kKt / 32; ++kk)
+            mma_pair(d, mn_sw128_desc(a + kk * 4096, kBoxBytes), mn_sw128_desc(b + kk * 4096, kBoxBytes),
+                     (ks | kk) != 0 ? 1u : 0u);
+          issued = true;
+          commit_pair(peer_addr(empty0 + 8 * s, 0));
+          commit_pair(peer_addr(empty0 + 8 * s, 1));
+        }
+        if (ok) {
+          commit_pair(peer_addr(tfull0 + 8 * acc, 0));
+          commit_pair(peer_addr(tfull0 + 8 * acc, 1));
+        }
+      }
+      if (leader && issued) {
+        // Every MMA of the pair has completed once mma_done fires.
+        commit_pair(peer_addr(mma_done, 0));
+        mbar_wait(mma_done, 0, nullptr);
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue --
+    const int ew = warp - 2;
+    const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31
+    const int m = quarter * 32 + lane;
+    const int c = m & 1;
+    const int p1 = (m >> 1) & 1;
+    const int il = m >> 2;
+    const bool copier = (ew == 0);
+    for (int i = 0;; ++i) {
+      const int slot = i % kSched;
+      const bool got = mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
+      Item t;
+      if (got) t = ring[slot];
+      if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      if (epi_any(!got)) {
+        if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
+        break;
+      }
+      if (ew == 0 && lane == 0) mbar_arrive(sempty0 + 8 * slot);
+      if (t.u >= p.total) break;
+      const int acc = i & 1;
+      const bool have = mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag);
+      if (epi_any(!have)) {
+        if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
+        break;
+      }
+      __syncwarp();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int rb = 2 * t.R + (int)rank;    // this CTA's 32-station row block
+      const long long i_glob = (long long)rb * kStations + il;
+      for (int h = 0; h < 2; ++h) {
+        const int cb = 2 * t.C + h;          // 32-station column block
+        if (cb > rb) continue;               // above the diagonal (uniform in the CTA)
+        if (h == 1) {
+          // the staging rows of column block 2C must have been read
+          if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          epi_barrier();
+        }
+        uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+        int jmax = job.n - cb * kStations;
+        if (jmax > kStations) jmax = kStations;
+        if (cb == rb && il + 1 < jmax) jmax = il + 1;
+        if (i_glob >= job.n) jmax = 0;
+#pragma unroll 1
+        for (int q = 0; q < kHalf / 32; ++q) {
+          uint32_t v[32];
+          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) +
+                        (uint32_t)(acc * kAccCols + h * kHalf + q * 32),
+                    v);
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int v0 = (int)v[4 * jj], v1 = (int)v[4 * jj + 1];
+            const int v2 = (int)v[4 * jj + 2], v3 = (int)v[4 * jj + 3];
+            const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
+            const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
+            const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
+            const long long im = c ? (long long)v2 - rb2 : (long long)ra - v1;
+            const int jl = q * 8 + jj;
+            if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        epi_barrier();
+        if (copier) {
+          // row `lane` of the staging block -> baselines (32 rb + lane, 32 cb .. )
+          const long long ig = (long long)rb * kStations + lane;
+          int cnt = job.n - cb * kStations;
+          if (cnt > kStations) cnt = kStations;
+          if (cb == rb && lane + 1 < cnt) cnt = lane + 1;
+          if (ig >= job.n) cnt = 0;
+          if (cnt > 0) {
+            int64_t *dst = job.state + ((long long)t.f * job.nbaseline + ig * (ig + 1) / 2 +
+                                        (long long)cb * kStations) * 8;
+            const uint32_t src = smem_u32(sstate + lane * kRowPitch);
+            if (job.store) bulk_store(dst, src, cnt * 64);
+            else bulk_reduce_add(dst, src, cnt * 64);
+          }
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+      }
+      // The accumulator has been read (or was not needed): release it.
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) remote_arrive(peer_addr(tempty0 + 8 * acc, 0));
+    }
+    if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  }
+
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  cluster_sync();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+}  // namespace tc2
+
+cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
+                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune) {
+  static int num_sms = 0;
+  static bool configured = false;
+  if (!configured) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tc2::xengine_tc2_kernel,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, tc2::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  tc2::Params p;
+  Job &j = p.job;
+  j.map = map;
+  const long long ntl = (4LL * s.n + 2 * tc2::kHalf - 1) / (2 * tc2::kHalf);
+  const long long npairs = ntl * (ntl + 1) / 2;
+  const int total_steps = (tcount + tc2::kKt - 1) / tc2::kKt;
+  int ksplit = tune.ksplit < 1 ? 1 : (tune.ksplit > total_steps ? total_steps : tune.ksplit);
+  const int per = (total_steps + ksplit - 1) / ksplit;
+  ksplit = (total_steps + per - 1) / per;
+  if ((long long)s.f * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
+  if (overwrite && ksplit > 1) {
+    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
+    if (e != cudaSuccess) return e;
+  }
+  j.state = state;
+  j.nbaseline = s.nbaseline;
+  j.n = s.n;
+  j.f = s.f;
+  j.t0 = t0;
+  j.total_steps = total_steps;
+  j.steps_per_split = per;
+  j.ksplit = ksplit;
+  j.npairs = (int)npairs;
+  j.items = (int)(s.f * npairs * ksplit);
+  j.item_begin = 0;
+  j.store = (overwrite && ksplit == 1) ? 1 : 0;
+  p.total = j.items;
+  p.err = err;
+  int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
+  if (clusters > p.total) clusters = p.total;
+  if (clusters < 1) clusters = 1;
+  tc2::xengine_tc2_kernel<<<2 * clusters, tc2::kThreads, tc2::kSmemBytes, st>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace xgpu

@@ -59,6 +59,9 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
                             const TcTuning &tune);
+// The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
+cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
+                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune);
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,

@@ -75,7 +75,7 @@ struct Internal {
   cudaEvent_t comp_done[2] = {nullptr, nullptr};
   int cur = 0;
   bool state_zero = true;
-  TcTuning tune{1, 0};   // tensor-core time splits and grid
+  TcTuning tune;   // tensor-core kernel, time splits and grid
 
   // tensor maps, cached by device pointer
   struct MapEntry {
@@ -359,6 +359,9 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
   in->cfg = cfg;
   in->sz = make_sizes(cfg);
   in->int_state = cfg.compute_type == XGPU_INT8;
+  // CTA-pair 256x256 tiles pay off once a channel has several of them; the
+  // autotuner (xgpuTune) revisits the choice per shape.
+  in->tune.wide = cfg.nstation >= 384 ? 1 : 0;
 
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -608,13 +611,14 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream) {
   return XGPU_OK;
 }
 
-int xgpuTune(XGPUContext *context, int ksplit, int grid) {
+int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   Internal *in = get(context);
   if (!in) return XGPU_NOT_INITIALIZED;
-  if (ksplit < 0 || grid < 0) return XGPU_INVALID_ARGUMENT;
+  if (ksplit < 0 || grid < 0 || pair < 0 || pair > 1) return XGPU_INVALID_ARGUMENT;
   if (ksplit > 0) {
     in->tune.ksplit = ksplit;
     in->tune.grid = grid;
+    in->tune.wide = pair;
     return XGPU_OK;
   }
   if (!in->int_state || in->cfg.engine != XGPU_ENGINE_TENSOR) return XGPU_OK;  // nothing to tune
@@ -643,8 +647,10 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, in->device);
   const int splits[] = {1, 2, 3, 4, 6, 8};
   int rc = XGPU_OK;
-  for (int ks : splits) {
-    TcTuning t{ks, 0};
+  for (int cand = 0; cand < 12; ++cand) {
+    TcTuning t;
+    t.ksplit = splits[cand % 6];
+    t.wide = cand / 6;
     auto run = [&]() {
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;

@@ -28,8 +28,9 @@ struct Job {
 };
 
 struct TcTuning {
-  int ksplit;             // time splits per tile (1 = none)
-  int grid;               // CTAs (0 = one per SM)
+  int ksplit = 1;         // time splits per tile (1 = none)
+  int grid = 0;           // CTAs (0 = one per SM)
+  int wide = 0;           // 1: CTA-pair kernel with 256x256 tiles (cta_group::2)
 };
 
 }  // namespace xgpu

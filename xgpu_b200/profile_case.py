@@ -23,6 +23,7 @@ def main():
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--ksplit", type=int, default=-1, help="-1: engine default, 0: autotune")
+    ap.add_argument("--pair", type=int, default=0, help="1: CTA-pair kernel (256x256 tiles)")
     ap.add_argument("--accumulate", action="store_true",
                     help="add into the integration (default: every call starts a new one)")
     ap.add_argument("--sigma", type=float, default=16.0)
@@ -33,8 +34,8 @@ def main():
     engine = "plain" if args.engine in ("plain", "fp32") else "tensor"
     c = xg.Correlator(args.n, args.f, args.t, ntimepipe=16, engine=engine, compute=compute,
                       output="int32" if compute == "int8" else "float32", order="tri")
-    if args.ksplit >= 0:
-        c.tune(args.ksplit, 0)
+    if args.ksplit >= 0 or args.pair:
+        c.tune(max(args.ksplit, 0) if args.ksplit != -1 else 1, 0, args.pair)
     stream = torch.cuda.Stream()
     c.set_stream(stream.cuda_stream)
     nbytes = int(c.info.vecLength) * 2
