@@ -313,6 +313,7 @@ typedef struct XGPUBatchImpl *XGPUBatch;
 
 #define XGPU_BATCH_AUTOTUNE 1  /* time split granularity and grid chosen by timing */
 #define XGPU_BATCH_GRAPH    2  /* capture the run once as a CUDA graph and replay it */
+#define XGPU_BATCH_PAIR     4  /* CTA-pair kernel, 256x256 tiles (without AUTOTUNE) */
 
 /* Plan a batch on `device`, run on `stream` (a cudaStream_t, NULL = legacy
  * default stream).  The job list is copied; the buffers must stay valid. */
@@ -322,7 +323,9 @@ int xgpuBatchCreate(XGPUBatch *batch, const XGPUBatchJob *jobs, int njobs, int d
 int xgpuBatchRun(XGPUBatch batch);
 /* Wait for queued runs; XGPU_CUDA_ERROR if a device wait timed out. */
 int xgpuBatchSync(XGPUBatch batch);
-/* Work items per run, CTAs, and samples-per-item stages chosen (0 = unsplit). */
+/* Work items per run, CTAs, and the time split chosen: max_steps >= 0 is the
+ * single-CTA kernel with that many 128-sample stages per item (0 = unsplit);
+ * max_steps < 0 is the CTA-pair kernel with -1 - max_steps stages per item. */
 int xgpuBatchInfo(XGPUBatch batch, int *work_items, int *grid, int *max_steps);
 void xgpuBatchDestroy(XGPUBatch batch);
 

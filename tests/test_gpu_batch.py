@@ -96,11 +96,13 @@ UNEVEN = [(32, 5, 256), (48, 1, 512), (64, 7, 2304), (96, 2, 768), (128, 3, 256)
           (16, 9, 4096), (256, 2, 1024), (80, 4, 8192), (32, 64, 256)]
 
 
-@pytest.mark.parametrize("autotune,graph", [(False, False), (True, False), (True, True)])
-def test_batch_matches_plain_job_by_job(xg, oracle_mod, autotune, graph):
+@pytest.mark.parametrize("autotune,graph,pair", [(False, False, False), (False, False, True),
+                                                 (False, True, True), (True, False, False),
+                                                 (True, True, False)])
+def test_batch_matches_plain_job_by_job(xg, oracle_mod, autotune, graph, pair):
     import torch
     jobs, keep = make_jobs(torch, oracle_mod, UNEVEN)
-    with xg.Batch(jobs, autotune=autotune, graph=graph) as b:
+    with xg.Batch(jobs, autotune=autotune, graph=graph, pair=pair) as b:
         b.run()
         b.sync()
         info = b.info()
@@ -123,7 +125,7 @@ def test_batch_accumulates(xg, oracle_mod):
     for j, (x, xd, st, n, f, t) in zip(jobs, keep):
         st.zero_()
         j["accumulate"] = 1
-    with xg.Batch(jobs, graph=True) as b:
+    with xg.Batch(jobs, graph=True, pair=True) as b:
         for _ in range(3):
             b.run()
         b.sync()

@@ -80,7 +80,7 @@ class XGPUBatchJob(ctypes.Structure):
     ]
 
 
-XGPU_BATCH_AUTOTUNE, XGPU_BATCH_GRAPH = 1, 2
+XGPU_BATCH_AUTOTUNE, XGPU_BATCH_GRAPH, XGPU_BATCH_PAIR = 1, 2, 4
 XGPU_SERVE_BATCHED, XGPU_SERVE_PLAIN_SERIAL = 0, 1
 
 
@@ -334,7 +334,7 @@ class Batch:
     pointer to the int64 triangular buffer), nstation, nfrequency, ntime and
     optionally accumulate (default 0)."""
 
-    def __init__(self, jobs, device=0, stream=None, autotune=False, graph=False):
+    def __init__(self, jobs, device=0, stream=None, autotune=False, graph=False, pair=False):
         arr = (XGPUBatchJob * len(jobs))()
         for a, j in zip(arr, jobs):
             a.device_input = j["input"]
@@ -342,7 +342,8 @@ class Batch:
             a.nstation, a.nfrequency, a.ntime = j["nstation"], j["nfrequency"], j["ntime"]
             a.accumulate = int(j.get("accumulate", 0))
         self.handle = ctypes.c_void_p()
-        flags = (XGPU_BATCH_AUTOTUNE if autotune else 0) | (XGPU_BATCH_GRAPH if graph else 0)
+        flags = ((XGPU_BATCH_AUTOTUNE if autotune else 0) | (XGPU_BATCH_GRAPH if graph else 0) |
+                 (XGPU_BATCH_PAIR if pair else 0))
         check("xgpuBatchCreate", lib().xgpuBatchCreate(ctypes.byref(self.handle), arr, len(jobs),
                                                        device, ctypes.c_void_p(stream), flags))
 

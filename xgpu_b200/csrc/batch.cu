@@ -38,6 +38,7 @@ struct XGPUBatchImpl {
   int total_items = 0;
   int grid = 0;
   int max_steps = 0;          // stages per work item (0: no time split)
+  int pair = 0;               // 1: CTA-pair kernel (256x256 tiles)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double tuned_ms = 0.0;
@@ -71,7 +72,7 @@ int splits_for(int t, int max_steps) {
 }
 
 // Build the job table for the given states (the plan's or scratch ones).
-int build_table(XGPUBatchImpl *b, const std::vector<int64_t *> &states, int max_steps,
+int build_table(XGPUBatchImpl *b, const std::vector<int64_t *> &states, int max_steps, int pair,
                 std::vector<Job> &table, int &total) {
   table.assign(b->jobs.size(), Job());
   long long begin = 0;
@@ -80,7 +81,7 @@ int build_table(XGPUBatchImpl *b, const std::vector<int64_t *> &states, int max_
     const Sizes &s = b->sizes[q];
     const int ks = splits_for(s.t, max_steps);
     if (tc_fill_job(&table[q], j.device_input, s, 0, s.t, states[q], j.accumulate ? 0 : 1, ks,
-                    (int)begin) != 0)
+                    (int)begin, pair) != 0)
       return XGPU_INVALID_ARGUMENT;
     begin += table[q].items;
     if (begin > 0x7fffffffLL) return XGPU_INVALID_ARGUMENT;
@@ -90,12 +91,16 @@ int build_table(XGPUBatchImpl *b, const std::vector<int64_t *> &states, int max_
 }
 
 // Queue one run of the batch on the plan's stream (no graph).
-int enqueue(XGPUBatchImpl *b, const std::vector<Job> &table, int total, Job *d_jobs, int grid) {
+int enqueue(XGPUBatchImpl *b, const std::vector<Job> &table, int total, Job *d_jobs, int grid,
+            int pair) {
   for (size_t q = 0; q < table.size(); ++q) {
     if (!b->jobs[q].accumulate && !table[q].store)
       BCHECK(cudaMemsetAsync(table[q].state, 0, (size_t)b->sizes[q].state_elems * 8, b->stream));
   }
-  BCHECK(launch_tc_batch(d_jobs, (int)table.size(), total, b->d_queue, b->d_err, grid, b->stream));
+  if (pair)
+    BCHECK(launch_tc2_batch(d_jobs, (int)table.size(), total, b->d_queue, b->d_err, grid, b->stream));
+  else
+    BCHECK(launch_tc_batch(d_jobs, (int)table.size(), total, b->d_queue, b->d_err, grid, b->stream));
   return XGPU_OK;
 }
 
@@ -107,7 +112,10 @@ int upload(XGPUBatchImpl *b, const std::vector<Job> &table, Job *d_jobs) {
 }
 
 std::mutex g_tune_mutex;
-std::map<std::vector<long long>, std::pair<int, int>> g_tune_cache;   // shape key -> (max_steps, grid)
+struct Tuned {
+  int max_steps, grid, pair;
+};
+std::map<std::vector<long long>, Tuned> g_tune_cache;   // shape key -> tuning
 
 std::vector<long long> shape_key(const XGPUBatchImpl *b) {
   std::vector<long long> k;
@@ -127,8 +135,9 @@ int autotune(XGPUBatchImpl *b) {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      b->max_steps = it->second.first;
-      b->grid = it->second.second;
+      b->max_steps = it->second.max_steps;
+      b->grid = it->second.grid;
+      b->pair = it->second.pair;
       return XGPU_OK;
     }
   }
@@ -154,20 +163,21 @@ int autotune(XGPUBatchImpl *b) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  int best_steps = 0, best_grid = sms;
+  int best_steps = 0, best_grid = sms, best_pair = 0;
   const int steps_cands[] = {0, 64, 32, 16, 8};
-  const int grid_cands[] = {sms, sms * 3 / 4};
+  const int grid_cands[] = {sms, (sms * 3 / 4) & ~1};
   std::vector<Job> table;
-  for (int ms : steps_cands) {
+  for (int cand = 0; cand < 10 && rc == XGPU_OK; ++cand) {
+    const int ms = steps_cands[cand % 5], pr = cand / 5;
     int total = 0;
-    if ((rc = build_table(b, scratch, ms, table, total)) != XGPU_OK) break;
+    if ((rc = build_table(b, scratch, ms, pr, table, total)) != XGPU_OK) break;
     if ((rc = upload(b, table, d_tab)) != XGPU_OK) break;
     for (int g : grid_cands) {
-      if (g < 1) continue;
-      if ((rc = enqueue(b, table, total, d_tab, g)) != XGPU_OK) break;   // warm
+      if (g < 2) continue;
+      if ((rc = enqueue(b, table, total, d_tab, g, pr)) != XGPU_OK) break;   // warm
       cudaEventRecord(e0, b->stream);
       for (int r = 0; r < 3; ++r)
-        if ((rc = enqueue(b, table, total, d_tab, g)) != XGPU_OK) break;
+        if ((rc = enqueue(b, table, total, d_tab, g, pr)) != XGPU_OK) break;
       cudaEventRecord(e1, b->stream);
       if (cudaEventSynchronize(e1) != cudaSuccess) {
         rc = XGPU_CUDA_ERROR;
@@ -179,9 +189,9 @@ int autotune(XGPUBatchImpl *b) {
         best = ms_run;
         best_steps = ms;
         best_grid = g;
+        best_pair = pr;
       }
     }
-    if (rc != XGPU_OK) break;
   }
   cudaStreamSynchronize(b->stream);
   cudaEventDestroy(e0);
@@ -191,9 +201,10 @@ int autotune(XGPUBatchImpl *b) {
   if (rc != XGPU_OK) return rc;
   b->max_steps = best_steps;
   b->grid = best_grid;
+  b->pair = best_pair;
   b->tuned_ms = best / 3.0;
   std::lock_guard<std::mutex> lock(g_tune_mutex);
-  g_tune_cache[key] = {best_steps, best_grid};
+  g_tune_cache[key] = {best_steps, best_grid, best_pair};
   return XGPU_OK;
 }
 
@@ -259,6 +270,7 @@ int xgpuBatchCreate(XGPUBatch *out, const XGPUBatchJob *jobs, int njobs, int dev
     return fail(XGPU_CUDA_ERROR);
   b->grid = num_sms(device);
   b->max_steps = 0;
+  b->pair = (flags & XGPU_BATCH_PAIR) ? 1 : 0;
   if (flags & XGPU_BATCH_AUTOTUNE) {
     int r = autotune(b);
     if (r != XGPU_OK) return fail(r);
@@ -266,7 +278,7 @@ int xgpuBatchCreate(XGPUBatch *out, const XGPUBatchJob *jobs, int njobs, int dev
   std::vector<int64_t *> states;
   for (const XGPUBatchJob &j : b->jobs) states.push_back((int64_t *)j.device_state);
   std::vector<Job> &table = b->table;
-  int r = build_table(b, states, b->max_steps, table, b->total_items);
+  int r = build_table(b, states, b->max_steps, b->pair, table, b->total_items);
   if (r != XGPU_OK) return fail(r);
   if ((r = upload(b, table, b->d_jobs)) != XGPU_OK) return fail(r);
   if (flags & XGPU_BATCH_GRAPH) {
@@ -277,7 +289,7 @@ int xgpuBatchCreate(XGPUBatch *out, const XGPUBatchJob *jobs, int njobs, int dev
     cudaStream_t keep = b->stream;
     b->stream = cs;
     bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    if (ok) ok = enqueue(b, table, b->total_items, b->d_jobs, b->grid) == XGPU_OK;
+    if (ok) ok = enqueue(b, table, b->total_items, b->d_jobs, b->grid, b->pair) == XGPU_OK;
     cudaGraph_t g = nullptr;
     ok = (cudaStreamEndCapture(cs, &g) == cudaSuccess) && ok;
     b->stream = keep;
@@ -300,7 +312,7 @@ int xgpuBatchRun(XGPUBatch b) {
     BCHECK(cudaGraphLaunch(b->exec, b->stream));
     return XGPU_OK;
   }
-  return enqueue(b, b->table, b->total_items, b->d_jobs, b->grid);
+  return enqueue(b, b->table, b->total_items, b->d_jobs, b->grid, b->pair);
 }
 
 int xgpuBatchSync(XGPUBatch b) {
@@ -322,7 +334,8 @@ int xgpuBatchInfo(XGPUBatch b, int *work_items, int *grid, int *max_steps) {
   if (!b) return XGPU_NOT_INITIALIZED;
   if (work_items) *work_items = b->total_items;
   if (grid) *grid = b->grid;
-  if (max_steps) *max_steps = b->max_steps;
+  // stages per item, negative when the CTA-pair kernel runs (-1: pairs, unsplit)
+  if (max_steps) *max_steps = b->pair ? -1 - b->max_steps : b->max_steps;
   return XGPU_OK;
 }
 

@@ -411,9 +411,10 @@ cudaError_t tc_check_device() {
 }
 
 int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount, int64_t *state,
-                int store, int ksplit, int item_begin) {
+                int store, int ksplit, int item_begin, int pair) {
   if (make_tc_tensor_map(&job->map, dev_in, s) != 0) return -1;
-  const long long ntl = (4LL * s.n + tc::kTile - 1) / tc::kTile;
+  const long long tile = pair ? 2 * tc::kTile : tc::kTile;
+  const long long ntl = (4LL * s.n + tile - 1) / tile;
   const long long npairs = ntl * (ntl + 1) / 2;
   const int total_steps = (tcount + tc::kKt - 1) / tc::kKt;
   if (ksplit < 1) ksplit = 1;

@@ -22,6 +22,7 @@
 // leader's "accumulator empty" barrier.  Every wait is bounded (as in
 // engine_tc.cu); both CTAs meet at a cluster barrier before releasing TMEM.
 #include <cudaTypedefs.h>
+#include <string.h>
 
 #include "internal.h"
 #include "tc_common.cuh"
@@ -49,22 +50,43 @@ constexpr int kThreads = 192;
 constexpr uint32_t kIdesc = i8_idesc(2 * kHalf, 2 * kHalf);
 
 struct Params {
-  Job job;     // npairs counts 256x256 tiles on or below the diagonal
-  int total;   // f * npairs * ksplit work items
+  Job job;             // the job when jobs == nullptr (npairs counts 256x256 tiles)
+  const Job *jobs;     // batched: job table in global memory, ordered by item_begin
+  int njobs;
+  int total;           // work items over all jobs
+  int *queue;          // dynamic work counter (zeroed before launch); nullptr: static stride
   int *err;
 };
 
+// A decoded work item, 64 bytes; the leader's scheduler writes it into both
+// CTAs' rings.
 struct Item {
-  int u;
-  int f, R, C;
+  int u;               // >= total: no more work
+  int f, R, C;         // channel and 256x256 tile (R >= C)
   int step0, nsteps;
+  int n, store, t0, pad;
+  long long nbaseline;
+  int64_t *state;
+  const CUtensorMap *map;
 };
+static_assert(sizeof(Item) == 64, "ring entries are copied as 8 words");
 
-__device__ __forceinline__ Item decode(const Job &j, int u) {
+__device__ __forceinline__ Item decode(const Params &p, int u) {
+  const Job *jp = &p.job;
+  if (p.jobs) {
+    int lo = 0, hi = p.njobs - 1;   // last job with item_begin <= u
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.jobs[mid].item_begin <= u) lo = mid; else hi = mid - 1;
+    }
+    jp = &p.jobs[lo];
+  }
+  const Job &j = *jp;
   Item it;
   it.u = u;
-  const int k = u % j.npairs;
-  const int rest = u / j.npairs;
+  const int v = u - j.item_begin;
+  const int k = v % j.npairs;
+  const int rest = v / j.npairs;
   const int split = rest % j.ksplit;
   it.f = rest / j.ksplit;
   int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
@@ -75,6 +97,13 @@ __device__ __forceinline__ Item decode(const Job &j, int u) {
   it.step0 = split * j.steps_per_split;
   const int ns = j.total_steps - it.step0;
   it.nsteps = ns < j.steps_per_split ? ns : j.steps_per_split;
+  it.n = j.n;
+  it.store = j.store;
+  it.t0 = j.t0;
+  it.pad = 0;
+  it.nbaseline = j.nbaseline;
+  it.state = j.state;
+  it.map = &j.map;
   return it;
 }
 
@@ -100,6 +129,43 @@ __device__ __forceinline__ void cluster_sync() {
 // cluster-scope fence on the arriving thread).
 __device__ __forceinline__ void remote_arrive(uint32_t cluster_bar) {
   asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+
+// Arrive with cluster-scope release: shared-memory stores the thread made in
+// the peer CTA before the arrival are visible to the peer's waiters.
+__device__ __forceinline__ void remote_arrive_release(uint32_t cluster_bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool try_wait_cluster(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// mbar_wait with cluster-scope acquire, for entries the other CTA wrote.
+__device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity,
+                                                  const volatile int *abort_flag) {
+  if (try_wait_cluster(bar, parity)) return true;
+  const uint64_t start = globaltimer_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (try_wait_cluster(bar, parity)) return true;
+    if ((it & 63u) == 0) {
+      if (abort_flag && *abort_flag) return false;
+      if (globaltimer_ns() - start > 2000000000ull) return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void st_cluster_u64(uint32_t cluster_addr, uint64_t v) {
+  asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(cluster_addr), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap *map,
@@ -147,7 +213,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   const uint32_t rank = cluster_rank();
   const bool leader = (rank == 0);
   const int cid = (int)(blockIdx.x >> 1), ncl = (int)(gridDim.x >> 1);
-  const Job &job = p.job;
 
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -167,7 +232,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     }
     for (int q = 0; q < kSched; ++q) {
       mbar_init(sfull0 + 8 * q, 1);
-      mbar_init(sempty0 + 8 * q, 2);
+      // leader's ring slot is free once the leader's MMA issuer and epilogue and
+      // the peer's producer and epilogue have copied the entry
+      mbar_init(sempty0 + 8 * q, 4);
     }
     mbar_init(mma_done, 1);
     *abort_flag = 0;
@@ -187,22 +254,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 
   if (warp == 0) {
     // ------------------------------------------------ scheduler + producer --
+    // The leader's lane takes the next item (queue or stride), decodes it once
+    // and publishes it to both CTAs' rings; the peer's producer follows its ring.
     if (lane == 0) {
-      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&job.map) : "memory");
+      if (!p.jobs && leader) asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.job.map) : "memory");
       uint32_t g = 0;
       bool ok = true;
       for (int i = 0; ok; ++i) {
         const int slot = i % kSched;
-        if (i >= kSched && !mbar_wait(sempty0 + 8 * slot, ((i / kSched) - 1) & 1, abort_flag)) {
-          fail(kErrTimeoutProducer);
-          break;
-        }
-        const int u = cid + i * ncl;
         Item t;
-        if (u < p.total) t = decode(job, u); else t.u = u;
-        ring[slot] = t;
-        mbar_arrive(sfull0 + 8 * slot);
-        if (u >= p.total) break;
+        if (leader) {
+          if (i >= kSched && !mbar_wait(sempty0 + 8 * slot, ((i / kSched) - 1) & 1, abort_flag)) {
+            fail(kErrTimeoutProducer);
+            break;
+          }
+          const int u = p.queue ? atomicAdd(p.queue, 1) : cid + i * ncl;
+          if (u < p.total) t = decode(p, u); else t.u = u;
+          ring[slot] = t;
+          const uint32_t remote = peer_addr(smem_u32(&ring[slot]), 1);
+#pragma unroll
+          for (int w = 0; w < 8; ++w) st_cluster_u64(remote + 8 * w, ((const uint64_t *)&t)[w]);
+          mbar_arrive(sfull0 + 8 * slot);
+          remote_arrive_release(peer_addr(sfull0 + 8 * slot, 1));
+        } else {
+          if (!mbar_wait_cluster(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)) {
+            fail(kErrTimeoutProducer);
+            break;
+          }
+          t = ring[slot];
+          remote_arrive(peer_addr(sempty0 + 8 * slot, 0));
+        }
+        if (t.u >= p.total) break;
         const bool diag = (t.R == t.C);
         const int rb = 2 * t.R + (int)rank, cbb = 2 * t.C + (int)rank;
         for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
@@ -218,15 +300,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           // The leader expects the bytes of both CTAs; the peer's loads may land
           // first (the transaction count then dips below zero until it does).
           if (leader) mbar_expect_tx(full0 + 8 * s, diag ? 2 * kBoxBytes : 4 * kBoxBytes);
-          const int z = job.t0 + (t.step0 + ks) * kKt;
-          tma_load_3d_pair(dst, &job.map, fbar, rb * kHalf, t.f, z);
-          if (!diag) tma_load_3d_pair(dst + kBoxBytes, &job.map, fbar, cbb * kHalf, t.f, z);
+          const int z = t.t0 + (t.step0 + ks) * kKt;
+          tma_load_3d_pair(dst, t.map, fbar, rb * kHalf, t.f, z);
+          if (!diag) tma_load_3d_pair(dst + kBoxBytes, t.map, fbar, cbb * kHalf, t.f, z);
         }
       }
     }
   } else if (warp == 1) {
     // --------------------------------------------------------------- MMA --
-    if (lane == 0) {
+    if (lane == 0 && leader) {
       uint32_t g = 0;
       bool ok = true;
       bool issued = false;
@@ -239,7 +321,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         const Item t = ring[slot];
         mbar_arrive(sempty0 + 8 * slot);
         if (t.u >= p.total) break;
-        if (!leader) continue;   // the leader issues the pair's MMAs
         const bool diag = (t.R == t.C);
         const int acc = i & 1;
         if (i >= 2 && !mbar_wait(tempty0 + 8 * acc, ((i >> 1) - 1) & 1, abort_flag)) {
@@ -271,7 +352,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           commit_pair(peer_addr(tfull0 + 8 * acc, 1));
         }
       }
-      if (leader && issued) {
+      if (issued) {
         // Every MMA of the pair has completed once mma_done fires.
         commit_pair(peer_addr(mma_done, 0));
         mbar_wait(mma_done, 0, nullptr);
@@ -288,7 +369,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     const bool copier = (ew == 0);
     for (int i = 0;; ++i) {
       const int slot = i % kSched;
-      const bool got = mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
+      const bool got = leader ? mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)
+                              : mbar_wait_cluster(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
       Item t;
       if (got) t = ring[slot];
       if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -296,7 +378,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
         break;
       }
-      if (ew == 0 && lane == 0) mbar_arrive(sempty0 + 8 * slot);
+      if (ew == 0 && lane == 0) {
+        if (leader) mbar_arrive(sempty0 + 8 * slot);
+        else remote_arrive(peer_addr(sempty0 + 8 * slot, 0));
+      }
       if (t.u >= p.total) break;
       const int acc = i & 1;
       const bool have = mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag);
@@ -317,10 +402,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           epi_barrier();
         }
         uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
-        int jmax = job.n - cb * kStations;
+        int jmax = t.n - cb * kStations;
         if (jmax > kStations) jmax = kStations;
         if (cb == rb && il + 1 < jmax) jmax = il + 1;
-        if (i_glob >= job.n) jmax = 0;
+        if (i_glob >= t.n) jmax = 0;
 #pragma unroll 1
         for (int q = 0; q < kHalf / 32; ++q) {
           uint32_t v[32];
@@ -344,15 +429,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         if (copier) {
           // row `lane` of the staging block -> baselines (32 rb + lane, 32 cb .. )
           const long long ig = (long long)rb * kStations + lane;
-          int cnt = job.n - cb * kStations;
+          int cnt = t.n - cb * kStations;
           if (cnt > kStations) cnt = kStations;
           if (cb == rb && lane + 1 < cnt) cnt = lane + 1;
-          if (ig >= job.n) cnt = 0;
+          if (ig >= t.n) cnt = 0;
           if (cnt > 0) {
-            int64_t *dst = job.state + ((long long)t.f * job.nbaseline + ig * (ig + 1) / 2 +
-                                        (long long)cb * kStations) * 8;
+            int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
+                                      (long long)cb * kStations) * 8;
             const uint32_t src = smem_u32(sstate + lane * kRowPitch);
-            if (job.store) bulk_store(dst, src, cnt * 64);
+            if (t.store) bulk_store(dst, src, cnt * 64);
             else bulk_reduce_add(dst, src, cnt * 64);
           }
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
@@ -419,11 +504,41 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   j.items = (int)(s.f * npairs * ksplit);
   j.item_begin = 0;
   j.store = (overwrite && ksplit == 1) ? 1 : 0;
+  p.jobs = nullptr;
+  p.njobs = 1;
+  p.queue = nullptr;
   p.total = j.items;
   p.err = err;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
   if (clusters > p.total) clusters = p.total;
   if (clusters < 1) clusters = 1;
+  tc2::xengine_tc2_kernel<<<2 * clusters, tc2::kThreads, tc2::kSmemBytes, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
+                             int grid, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tc2::xengine_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc2::kSmemBytes);
+  if (e != cudaSuccess) return e;
+  if (queue) {
+    e = cudaMemsetAsync(queue, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+  }
+  tc2::Params p;
+  memset(&p.job, 0, sizeof(p.job));
+  p.jobs = dev_jobs;
+  p.njobs = njobs;
+  p.total = total_items;
+  p.queue = queue;
+  p.err = err;
+  int clusters = (grid > 0 ? grid : sms) / 2;
+  if (clusters > total_items) clusters = total_items;
+  if (clusters < 1) return cudaSuccess;
   tc2::xengine_tc2_kernel<<<2 * clusters, tc2::kThreads, tc2::kSmemBytes, st>>>(p);
   return cudaGetLastError();
 }

@@ -67,9 +67,13 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
                             int grid, cudaStream_t st);
 // Fill a job for samples [t0, t0+tcount) of dev_in (sizes s).  store=1 asks for
-// plain stores (only honoured without time splits).  Returns 0 on success.
+// plain stores (only honoured without time splits); pair=1 cuts it into the
+// 256x256 tiles of the CTA-pair kernel.  Returns 0 on success.
 int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount, int64_t *state,
-                int store, int ksplit, int item_begin);
+                int store, int ksplit, int item_begin, int pair);
+// The CTA-pair kernel over a device job table filled with pair = 1.
+cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
+                             int grid, cudaStream_t st);
 // Encodes the 3-D tensor map {x: 4n bytes, y: f, z: t} over a device input
 // buffer.  Returns 0 on success.
 int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);

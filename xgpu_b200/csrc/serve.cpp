@@ -8,7 +8,8 @@
 //    their integration state resident until their last dump;
 //  * every step, takes the available blocks (up to four) of every admitted
 //    request -- requests that arrived while others run join the next step --
-//    and runs all of them in ONE launch of the persistent tensor-core kernel
+//    and runs all of them in ONE launch of the persistent CTA-pair tensor-core
+//    kernel (engine_tc2.cu, 256x256 tiles)
 //    through a device job table, so the work of different requests overlaps
 //    on the GPU;  blocks of one request in one step add their partial sums
 //    exactly (bulk reduce-add);
@@ -404,7 +405,7 @@ extern "C" int xgpuServeRun(const XGPUServeJob *jobs, int njobs, const XGPUServe
             } else {
               Job &jb = tab[nent++];
               if (tc_fill_job(&jb, x, a.s, 0, a.s.t, (int64_t *)a.state,
-                              (first && rq.second == 1) ? 1 : 0, 1, items) != 0) {
+                              (first && rq.second == 1) ? 1 : 0, 1, items, 1) != 0) {
                 rc = XGPU_CUDA_ERROR;
                 goto done;
               }
@@ -417,7 +418,7 @@ extern "C" int xgpuServeRun(const XGPUServeJob *jobs, int njobs, const XGPUServe
         if (!plain) {
           Job *dtab = d_tables + (size_t)table_slot * max_table;
           SCHECK(cudaMemcpyAsync(dtab, tab, sizeof(Job) * nent, cudaMemcpyHostToDevice, s_step));
-          SCHECK(launch_tc_batch(dtab, nent, items, d_queue + table_slot, d_err, sms, s_step));
+          SCHECK(launch_tc2_batch(dtab, nent, items, d_queue + table_slot, d_err, sms, s_step));
         }
         table_slot = (table_slot + 1) % kTables;
         for (const auto &rq : ready) {

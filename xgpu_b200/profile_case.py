@@ -4,12 +4,14 @@
                                      [--reps 5] [--warmup 3] [--ksplit K] [--accumulate]
 
 Prints one JSON line: milliseconds per xgpuCudaXengineDevice call (CUDA
-events on the engine's stream) and X-engine TOPS (16*F*T*N(N+1) ops per
-call).  Useful to size a deployment and as a small, self-contained case for
+events on the engine's stream), X-engine TOPS (16*F*T*N(N+1) ops per call)
+and the host time to queue one call (when it approaches the device time, the
+caller, not the GPU, sets the pace).  Useful to size a deployment and as a small, self-contained case for
 profilers.
 """
 import argparse
 import json
+import time
 
 import xgpu_b200 as xg
 
@@ -48,16 +50,18 @@ def main():
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    h0 = time.perf_counter()
     for _ in range(args.reps):
         if not args.accumulate:
             c.clear()
         c.run_device(x.data_ptr(), xg.SYNCOP_NONE)
+    host_ms = (time.perf_counter() - h0) * 1e3 / args.reps
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.reps
     ops = xg.ops_per_integration(args.n, args.f, args.t)
     print(json.dumps({"engine": c.engine_name, "n": args.n, "f": args.f, "t": args.t,
-                      "ms": ms, "tops": ops / (ms * 1e-3) / 1e12,
+                      "ms": ms, "tops": ops / (ms * 1e-3) / 1e12, "host_enqueue_ms": host_ms,
                       "accumulate": args.accumulate}))
     c.close()
 
