@@ -294,6 +294,14 @@ int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGP
  * and the fastest setting is kept. */
 int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);
 
+/* Extension for testing a caller's error handling.  While enabled, the
+ * tensor-core engine of this context issues no input loads, so its bounded
+ * device waits expire (about 2 s per launch) instead of completing: the next
+ * synchronising call returns XGPU_CUDA_ERROR, the integration in progress is
+ * invalid, and once disabled the context works normally (clear it first).
+ * Nothing faults or hangs. */
+int xgpuInjectTimeout(XGPUContext *context, int enable);
+
 /* ---- Extension: batches of uneven subarrays in one launch ---------------- */
 /* One subarray: its own station, channel and sample counts, its input
  * ([t][f][s][p][c] int8, 16-byte aligned) and its int64 integration buffer

@@ -1,0 +1,31 @@
+"""Failure detection without a GPU fault.
+
+Every wait of the tensor-core kernels is bounded (about 2 s); when one
+expires the kernel records an error code, the other roles stop, TMEM is
+released and the kernel returns.  xgpuInjectTimeout makes the engine withhold
+its input loads so the waits expire on purpose (a flag nothing sets); the
+host must report XGPU_CUDA_ERROR and the context must keep working."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("pair", [0, 1])
+def test_expired_device_wait_is_reported_and_recoverable(xg, oracle_mod, pair):
+    n, f, t = 64, 2, 1024
+    x = oracle_mod.gaussian_input(n, f, t, seed=5)
+    with xg.Correlator(n, f, t, engine="tensor") as c:
+        c.tune(1, 0, pair)
+        c.set_input(x)
+        assert xg.lib().xgpuInjectTimeout(ctypes.byref(c.ctx), 1) == 0
+        with pytest.raises(xg.XGPUError) as err:
+            c.run(xg.SYNCOP_SYNC_COMPUTE)
+        assert err.value.code == xg.XGPU_CUDA_ERROR
+        assert xg.lib().xgpuInjectTimeout(ctypes.byref(c.ctx), 0) == 0
+        c.clear()
+        c.run(xg.SYNCOP_DUMP)
+        got = c.dump_int64()
+    assert np.array_equal(got, oracle_mod.xengine_i64(x, n, f, t))

@@ -162,6 +162,7 @@ _PROTOTYPES = [
     ("xgpuBatchInfo", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("xgpuBatchDestroy", None, [ctypes.c_void_p]),
+    ("xgpuInjectTimeout", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_int]),
     ("xgpuServeRun", ctypes.c_int, [ctypes.POINTER(XGPUServeJob), ctypes.c_int,
                                     ctypes.POINTER(XGPUServeOptions),
                                     ctypes.POINTER(XGPUServeStats),

@@ -68,6 +68,7 @@ struct Params {
   int total;           // work items over all jobs
   int *queue;          // dynamic work counter (zeroed before launch); nullptr: static stride
   int *err;
+  int stall;           // test switch: issue no loads (the waits on them expire)
 };
 
 // A decoded work item.  The scheduler decodes each item once and publishes it
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
     // ------------------------------------------------ scheduler + producer --
     if (lane == 0) {
       if (!p.jobs) asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.single.map) : "memory");
-      uint32_t g = 0;
+      uint32_t g = 0, g_loaded = 0;
       bool ok = true;
       for (int i = 0; ok; ++i) {
         const int slot = i % kSched;
@@ -222,15 +223,17 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
             ok = false;
             break;
           }
+          if (p.stall) continue;
           const uint32_t dst = stage0 + s * kStageBytes;
           mbar_expect_tx(full0 + 8 * s, diag ? kBoxBytes : 2 * kBoxBytes);
           const int z = t.t0 + (t.step0 + ks) * kKt;
           tma_load_3d(dst, map, full0 + 8 * s, t.tr * kTile, t.f, z);
           if (!diag) tma_load_3d(dst + kBoxBytes, map, full0 + 8 * s, t.tc * kTile, t.f, z);
+          g_loaded = g + 1;
         }
       }
       // Loads still in flight land before the CTA leaves (a no-op normally).
-      for (uint32_t q = (g > (uint32_t)kStages ? g - kStages : 0); q < g; ++q)
+      for (uint32_t q = (g_loaded > (uint32_t)kStages ? g_loaded - kStages : 0); q < g_loaded; ++q)
         mbar_wait(full0 + 8 * (q % kStages), (q / kStages) & 1, nullptr);
     }
   } else if (warp == 1) {
@@ -490,6 +493,7 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
   p.total = j.items;
   p.queue = nullptr;
   p.err = err;
+  p.stall = tune.stall;
   int grid = tune.grid > 0 ? tune.grid : sms;
   if (grid > p.total) grid = p.total;
   tc::xengine_tc_kernel<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(p);
@@ -514,6 +518,7 @@ cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int
   p.total = total_items;
   p.queue = queue;
   p.err = err;
+  p.stall = 0;
   if (grid <= 0) grid = sms;
   if (grid > total_items) grid = total_items;
   if (grid < 1) return cudaSuccess;

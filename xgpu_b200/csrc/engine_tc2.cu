@@ -56,6 +56,7 @@ struct Params {
   int total;           // work items over all jobs
   int *queue;          // dynamic work counter (zeroed before launch); nullptr: static stride
   int *err;
+  int stall;           // test switch: issue no loads (the waits on them expire)
 };
 
 // A decoded work item, 64 bytes; the leader's scheduler writes it into both
@@ -295,6 +296,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             ok = false;
             break;
           }
+          if (p.stall) continue;
           const uint32_t dst = stage0 + s * kStageBytes;
           const uint32_t fbar = peer_addr(full0 + 8 * s, 0);
           // The leader expects the bytes of both CTAs; the peer's loads may land
@@ -509,6 +511,7 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   p.queue = nullptr;
   p.total = j.items;
   p.err = err;
+  p.stall = tune.stall;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
   if (clusters > p.total) clusters = p.total;
   if (clusters < 1) clusters = 1;
@@ -536,6 +539,7 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
   p.total = total_items;
   p.queue = queue;
   p.err = err;
+  p.stall = 0;
   int clusters = (grid > 0 ? grid : sms) / 2;
   if (clusters > total_items) clusters = total_items;
   if (clusters < 1) return cudaSuccess;

@@ -680,6 +680,13 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   return check_device_error(in);
 }
 
+int xgpuInjectTimeout(XGPUContext *context, int enable) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  in->tune.stall = enable ? 1 : 0;
+  return XGPU_OK;
+}
+
 int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long long seed,
                        double sigma, int device) {
   if (!device_out || kind < 0 || kind > 2 || (kind == 0 && !(sigma > 0))) return XGPU_INVALID_ARGUMENT;

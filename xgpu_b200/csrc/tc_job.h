@@ -31,6 +31,7 @@ struct TcTuning {
   int ksplit = 1;         // time splits per tile (1 = none)
   int grid = 0;           // CTAs (0 = one per SM)
   int wide = 0;           // 1: CTA-pair kernel with 256x256 tiles (cta_group::2)
+  int stall = 0;          // test switch: withhold input loads so the bounded waits expire
 };
 
 }  // namespace xgpu
