@@ -242,7 +242,8 @@ int xgpuContextInfo(XGPUContext *context, XGPUInfo *info);
 /* xgpuCudaXengine on input that is already in device memory (same layout
  * and size as array_h would hold; 16-byte aligned).  The caller keeps the
  * buffer unchanged until the call's work is done (any syncOp but NONE, or a
- * later synchronising call). */
+ * later synchronising call).  The input must be complete when the call is
+ * made, or be produced on the stream given to xgpuSetComputeStream. */
 int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int syncOp);
 
 /* Exact dump: the integration as int64 in triangular order,
@@ -286,7 +287,10 @@ int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGP
 
 /* Kernel, time splits and grid of the tensor-core engine for this context.
  * pair = 0 runs one CTA per 128x128 tile of the Gram matrix; pair = 1 runs
- * CTA pairs (tcgen05 cta_group::2) on 256x256 tiles.  ksplit >= 1 splits
+ * CTA pairs (tcgen05 cta_group::2) on 256x256 tiles; pair = 2 runs single CTAs
+ * that each take an equal share of all (tile, 128-sample) steps ("stream-K":
+ * tiles cut between CTAs add their parts exactly) when a call adds into
+ * existing sums, and 128x128 tiles otherwise.  ksplit >= 1 splits
  * every tile's samples into that many items whose partial sums are added
  * exactly in the integration buffer; grid is the number of CTAs (0 = one per
  * SM).  ksplit = 0 autotunes all three now: the engine is timed on synthetic

@@ -64,6 +64,22 @@ def test_pair_kernel_parity(xg, oracle_mod, n, f, t):
         assert np.array_equal(got, (2 * exact).astype(np.int32))
 
 
+@pytest.mark.parametrize("n,f,t,grid", [(256, 10, 1024, 0), (64, 3, 1024 + 384, 7), (48, 2, 128, 5),
+                                        (128, 5, 2048, 148), (16, 1, 64, 0)])
+def test_stream_k_shares_are_exact(xg, oracle_mod, n, f, t, grid):
+    """Stream-K: CTAs take equal shares of all (tile, step) pairs; tiles cut
+    between CTAs add up exactly.  The first call after a clear stores (plain
+    tiles), the following ones add with stream-K shares."""
+    x = oracle_mod.gaussian_input(n, f, t, seed=3 * n + t, sigma=28.0)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor") as c:
+        c.tune(1, grid, 2)
+        c.set_input(x)
+        for _ in range(3):
+            c.run(xg.SYNCOP_SYNC_COMPUTE)
+        assert np.array_equal(c.dump_int64(), 3 * exact)
+
+
 def test_pair_kernel_small_grid_and_autotune(xg, oracle_mod):
     n, f, t = 256, 6, 2048
     x = oracle_mod.gaussian_input(n, f, t, seed=77)

@@ -261,3 +261,43 @@ def test_reference_api_default_context(xg, oracle_mod):
     exact = oracle_mod.xengine_i64(x, info.nstation, info.nfrequency, info.ntime)
     assert np.array_equal(m[: exact.size], exact.astype(np.float32))
     L.xgpuFree(ctypes.byref(ctx))
+
+
+@pytest.mark.parametrize("fmt", ["packed4", "dp4a_swizzled"])
+def test_converted_inputs_back_to_back(xg, oracle_mod, fmt):
+    """Several calls in flight: each call's input conversion runs on its own
+    stream into one of two buffers, under the previous call's correlation."""
+    n, f, t = 96, 3, 1024
+    raws, feeds = [], []
+    for s in range(4):
+        if fmt == "packed4":
+            p = oracle_mod.generate(t * f * n * 2, 1, 50 + s)
+            raws.append(oracle_mod.unpack4(p))
+            feeds.append(p)
+        else:
+            x = oracle_mod.gaussian_input(n, f, t, seed=50 + s)
+            raws.append(x)
+            feeds.append(oracle_mod.swizzle(x, n, f, t))
+    with xg.Correlator(n, f, t, engine="tensor", input_format=fmt) as c:
+        for q, feed in enumerate(feeds):
+            c.set_input(feed)
+            c.run(xg.SYNCOP_SYNC_TRANSFER if q < 3 else xg.SYNCOP_DUMP)
+        got = c.dump_int64()
+    assert np.array_equal(got, oracle_mod.xengine_i64(np.concatenate(raws), n, f, 4 * t))
+
+
+def test_converted_device_input_on_caller_stream(xg, oracle_mod):
+    import torch
+    n, f, t = 64, 2, 512
+    stream = torch.cuda.Stream()
+    with xg.Correlator(n, f, t, engine="tensor", input_format="packed4") as c:
+        c.set_stream(stream.cuda_stream)
+        want = np.zeros(f * n * (n + 1) // 2 * 8, dtype=np.int64)
+        for s in range(3):
+            p = oracle_mod.generate(t * f * n * 2, 1, 70 + s)
+            with torch.cuda.stream(stream):
+                d = torch.from_numpy(p).to("cuda", non_blocking=False)
+                c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+                stream.synchronize()
+            oracle_mod.xengine_i64(oracle_mod.unpack4(p), n, f, t, acc=want)
+        assert np.array_equal(c.dump_int64(), want)

@@ -303,7 +303,8 @@ class Correlator:
 
     def tune(self, ksplit=0, grid=0, pair=0):
         """Tensor-core kernel choice: ksplit=0 autotunes; else fixed time splits,
-        grid (0 = one CTA per SM) and kernel (pair=1: CTA pairs, 256x256 tiles)."""
+        grid (0 = one CTA per SM) and kernel (pair=1: CTA pairs, 256x256 tiles;
+        pair=2: single CTAs with stream-K shares for accumulating calls)."""
         return check("xgpuTune", lib().xgpuTune(ctypes.byref(self.ctx), ksplit, grid, pair))
 
     def set_stream(self, stream_handle):

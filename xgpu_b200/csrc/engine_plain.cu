@@ -110,7 +110,7 @@ __device__ __forceinline__ void to_words(const uint8_t *raw, int4 *words) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads) xengine_dp4a_kernel(const Params p) {
+__global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const Params p) {
   __shared__ __align__(16) uint8_t raw[2][2][kRawPanel];
   __shared__ __align__(16) int4 words[2][kWordPanel / 16];
 
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) xengine_dp4a_kernel(const Params p) 
     __syncthreads();
     const int4 *rw = words[0];
     const int4 *cw = diag ? words[0] : words[1];
-#pragma unroll 2
+#pragma unroll 1
     for (int g = 0; g < kGroups; ++g) {
       int4 r[2], c[2];
       r[0] = rw[g * kBlk + ty];

@@ -69,6 +69,7 @@ struct Params {
   int *queue;          // dynamic work counter (zeroed before launch); nullptr: static stride
   int *err;
   int stall;           // test switch: issue no loads (the waits on them expire)
+  int streamk;         // single job: each CTA takes an equal share of all (tile, stage) steps
 };
 
 // A decoded work item.  The scheduler decodes each item once and publishes it
@@ -197,19 +198,43 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       if (!p.jobs) asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.single.map) : "memory");
       uint32_t g = 0, g_loaded = 0;
       bool ok = true;
+      // Stream-K: CTA b covers steps [b*W/G, (b+1)*W/G) of the W = items x
+      // stages of the job, cutting tiles where the ranges meet; the pieces of
+      // a cut tile add up exactly in the integration buffer (reduce-add).
+      const long long sk_w = p.streamk ? (long long)p.total * p.single.total_steps : 0;
+      long long sk_pos = p.streamk ? sk_w * blockIdx.x / gridDim.x : 0;
+      const long long sk_end = p.streamk ? sk_w * (blockIdx.x + 1) / gridDim.x : 0;
       for (int i = 0; ok; ++i) {
         const int slot = i % kSched;
         if (i >= kSched && !mbar_wait(sempty0 + 8 * slot, ((i / kSched) - 1) & 1, abort_flag)) {
           fail(kErrTimeoutProducer);
           break;
         }
-        const int u = p.queue ? atomicAdd(p.queue, 1) : (int)blockIdx.x + i * (int)gridDim.x;
         Item t;
-        if (u < p.total) {
-          t = decode_item(p, u);
+        if (p.streamk) {
+          if (sk_pos < sk_end) {
+            const int ts = p.single.total_steps;
+            const int item = (int)(sk_pos / ts);
+            const int s0 = (int)(sk_pos % ts);
+            const long long left = sk_end - sk_pos;
+            const int ns = (int)(ts - s0 < left ? ts - s0 : left);
+            t = decode_item(p, item);
+            t.step0 = s0;
+            t.nsteps = ns;
+            t.store = (s0 == 0 && ns == ts) ? t.store : 0;
+            sk_pos += ns;
+          } else {
+            t.u = p.total;
+          }
         } else {
-          t.u = u;
+          const int u = p.queue ? atomicAdd(p.queue, 1) : (int)blockIdx.x + i * (int)gridDim.x;
+          if (u < p.total) {
+            t = decode_item(p, u);
+          } else {
+            t.u = u;
+          }
         }
+        const int u = t.u;
         ring[slot] = t;
         mbar_arrive(sfull0 + 8 * slot);   // release: the entry is visible to the waiters
         if (u >= p.total) break;
@@ -494,6 +519,8 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
   p.queue = nullptr;
   p.err = err;
   p.stall = tune.stall;
+  // Stream-K only when every piece adds into existing sums (no stores).
+  p.streamk = (tune.streamk && !j.store && ksplit == 1) ? 1 : 0;
   int grid = tune.grid > 0 ? tune.grid : sms;
   if (grid > p.total) grid = p.total;
   tc::xengine_tc_kernel<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(p);
@@ -519,6 +546,7 @@ cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int
   p.queue = queue;
   p.err = err;
   p.stall = 0;
+  p.streamk = 0;
   if (grid <= 0) grid = sms;
   if (grid > total_items) grid = total_items;
   if (grid < 1) return cudaSuccess;

@@ -63,7 +63,16 @@ struct Internal {
   bool int_state = true;  // int64 buffer (integer engines) or float (FP32)
 
   void *d_in[2] = {nullptr, nullptr};  // one call's input, as supplied
-  int8_t *d_conv = nullptr;            // int8 [t][f][s][p][c] after conversion
+  // Packed 4+4-bit and DP4A-swizzled input is converted to int8
+  // [t][f][s][p][c] on its own stream into one of two buffers, so the
+  // conversion of call k+1 runs under the engine of call k.
+  int8_t *d_conv[2] = {nullptr, nullptr};
+  cudaStream_t s_conv = nullptr;
+  cudaEvent_t conv_done[2] = {nullptr, nullptr};
+  cudaEvent_t conv_free[2] = {nullptr, nullptr};   // engine that read d_conv[k] finished
+  bool conv_used[2] = {false, false};
+  int conv_cur = 0;
+  cudaEvent_t caller_ev = nullptr;                 // orders caller-stream work before a conversion
   void *d_state = nullptr;             // integration buffer
   void *d_out = nullptr;               // formatted dump
   int *d_err = nullptr;                // device error word
@@ -165,7 +174,16 @@ int free_device(Internal *in) {
   }
   if (in->s_copy) cudaStreamDestroy(in->s_copy);
   if (in->s_own) cudaStreamDestroy(in->s_own);
-  if (in->d_conv) cudaFree(in->d_conv);
+  for (int k = 0; k < 2; ++k) {
+    if (in->d_conv[k]) cudaFree(in->d_conv[k]);
+    if (in->conv_done[k]) cudaEventDestroy(in->conv_done[k]);
+    if (in->conv_free[k]) cudaEventDestroy(in->conv_free[k]);
+  }
+  if (in->s_conv) {
+    cudaStreamSynchronize(in->s_conv);
+    cudaStreamDestroy(in->s_conv);
+  }
+  if (in->caller_ev) cudaEventDestroy(in->caller_ev);
   if (in->d_state) cudaFree(in->d_state);
   if (in->d_out) cudaFree(in->d_out);
   if (in->d_err) cudaFree(in->d_err);
@@ -209,15 +227,31 @@ const CUtensorMap *tensor_map(Internal *in, const void *ptr) {
 }
 
 // Queue the engine over one call's device input (any format) on s_comp.
-int run_engine(Internal *in, const void *d_input) {
+// input_ready, when given, is the event after which the input is complete
+// (the host-to-device copy); converted formats wait for it on s_conv.
+int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   const Sizes &s = in->sz;
   const int8_t *x = (const int8_t *)d_input;
-  if (in->cfg.input_format == XGPU_INPUT_PACKED4) {
-    XGPU_CHECK(launch_unpack4((const uint8_t *)d_input, in->d_conv, s.vec_length, in->s_comp));
-    x = in->d_conv;
-  } else if (in->cfg.input_format == XGPU_INPUT_DP4A_SWIZZLED) {
-    XGPU_CHECK(launch_unswizzle_dp4a((const int8_t *)d_input, in->d_conv, s, in->s_comp));
-    x = in->d_conv;
+  int conv = -1;
+  if (in->cfg.input_format != XGPU_INPUT_INT8) {
+    conv = in->conv_cur;
+    in->conv_cur ^= 1;
+    if (in->conv_used[conv]) XGPU_CHECK(cudaStreamWaitEvent(in->s_conv, in->conv_free[conv], 0));
+    if (input_ready) XGPU_CHECK(cudaStreamWaitEvent(in->s_conv, input_ready, 0));
+    if (in->s_comp != in->s_own) {
+      // The caller's stream may have produced the input: convert after it.
+      XGPU_CHECK(cudaEventRecord(in->caller_ev, in->s_comp));
+      XGPU_CHECK(cudaStreamWaitEvent(in->s_conv, in->caller_ev, 0));
+    }
+    if (in->cfg.input_format == XGPU_INPUT_PACKED4)
+      XGPU_CHECK(launch_unpack4((const uint8_t *)d_input, in->d_conv[conv], s.vec_length, in->s_conv));
+    else
+      XGPU_CHECK(launch_unswizzle_dp4a((const int8_t *)d_input, in->d_conv[conv], s, in->s_conv));
+    XGPU_CHECK(cudaEventRecord(in->conv_done[conv], in->s_conv));
+    XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->conv_done[conv], 0));
+    x = in->d_conv[conv];
+  } else if (input_ready) {
+    XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, input_ready, 0));
   }
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
@@ -241,6 +275,10 @@ int run_engine(Internal *in, const void *d_input) {
     }
   }
   in->state_zero = false;
+  if (conv >= 0) {
+    XGPU_CHECK(cudaEventRecord(in->conv_free[conv], in->s_comp));
+    in->conv_used[conv] = true;
+  }
   return XGPU_OK;
 }
 
@@ -399,7 +437,8 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
       cudaMalloc(&in->d_err, sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&in->h_err, sizeof(int)) != cudaSuccess ||
       (cfg.input_format != XGPU_INPUT_INT8 &&
-       cudaMalloc(&in->d_conv, (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess)) {
+       (cudaMalloc(&in->d_conv[0], (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess ||
+        cudaMalloc(&in->d_conv[1], (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess))) {
     cudaGetLastError();
     return fail(XGPU_OUT_OF_MEMORY);
   }
@@ -409,9 +448,14 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
   in->s_comp = in->s_own;
   for (int b = 0; b < 2; ++b) {
     if (cudaEventCreateWithFlags(&in->copy_done[b], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&in->comp_done[b], cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&in->comp_done[b], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&in->conv_done[b], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&in->conv_free[b], cudaEventDisableTiming) != cudaSuccess)
       return fail(XGPU_CUDA_ERROR);
   }
+  if (cudaStreamCreateWithFlags(&in->s_conv, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&in->caller_ev, cudaEventDisableTiming) != cudaSuccess)
+    return fail(XGPU_CUDA_ERROR);
   if (cudaMemsetAsync(in->d_err, 0, sizeof(int), in->s_comp) != cudaSuccess ||
       cudaMemsetAsync(in->d_state, 0, state_bytes, in->s_comp) != cudaSuccess ||
       cudaStreamSynchronize(in->s_comp) != cudaSuccess)
@@ -554,8 +598,7 @@ int xgpuCudaXengine(XGPUContext *context, int syncOp) {
   XGPU_CHECK(cudaMemcpyAsync(in->d_in[b], context->array_h + context->input_offset,
                              (size_t)in->sz.input_bytes, cudaMemcpyHostToDevice, in->s_copy));
   XGPU_CHECK(cudaEventRecord(in->copy_done[b], in->s_copy));
-  XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->copy_done[b], 0));
-  int r = run_engine(in, in->d_in[b]);
+  int r = run_engine(in, in->d_in[b], in->copy_done[b]);
   if (r != XGPU_OK) return r;
   XGPU_CHECK(cudaEventRecord(in->comp_done[b], in->s_comp));
   return finish_call(context, in, syncOp);
@@ -567,7 +610,7 @@ int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int sy
   if (!device_input || ((uintptr_t)device_input & 15) != 0) return XGPU_INVALID_ARGUMENT;
   if (syncOp < SYNCOP_NONE || syncOp > SYNCOP_SYNC_COMPUTE) return XGPU_INVALID_ARGUMENT;
   XGPU_CHECK(cudaSetDevice(in->device));
-  int r = run_engine(in, device_input);
+  int r = run_engine(in, device_input, nullptr);
   if (r != XGPU_OK) return r;
   return finish_call(context, in, syncOp);
 }
@@ -614,11 +657,12 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream) {
 int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   Internal *in = get(context);
   if (!in) return XGPU_NOT_INITIALIZED;
-  if (ksplit < 0 || grid < 0 || pair < 0 || pair > 1) return XGPU_INVALID_ARGUMENT;
+  if (ksplit < 0 || grid < 0 || pair < 0 || pair > 2) return XGPU_INVALID_ARGUMENT;
   if (ksplit > 0) {
     in->tune.ksplit = ksplit;
     in->tune.grid = grid;
-    in->tune.wide = pair;
+    in->tune.wide = pair == 1 ? 1 : 0;
+    in->tune.streamk = pair == 2 ? 1 : 0;
     return XGPU_OK;
   }
   if (!in->int_state || in->cfg.engine != XGPU_ENGINE_TENSOR) return XGPU_OK;  // nothing to tune
@@ -647,10 +691,11 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, in->device);
   const int splits[] = {1, 2, 3, 4, 6, 8};
   int rc = XGPU_OK;
-  for (int cand = 0; cand < 12; ++cand) {
+  for (int cand = 0; cand < 13; ++cand) {
     TcTuning t;
-    t.ksplit = splits[cand % 6];
-    t.wide = cand / 6;
+    t.ksplit = cand < 12 ? splits[cand % 6] : 1;
+    t.wide = cand < 12 ? cand / 6 : 0;
+    t.streamk = cand == 12 ? 1 : 0;
     auto run = [&]() {
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;

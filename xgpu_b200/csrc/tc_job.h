@@ -32,6 +32,8 @@ struct TcTuning {
   int grid = 0;           // CTAs (0 = one per SM)
   int wide = 0;           // 1: CTA-pair kernel with 256x256 tiles (cta_group::2)
   int stall = 0;          // test switch: withhold input loads so the bounded waits expire
+  int streamk = 0;        // single-CTA kernel: equal shares of all tile steps per CTA
+                          // (used for launches that add into existing sums)
 };
 
 }  // namespace xgpu
