@@ -154,9 +154,9 @@ def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, 
                       device=torch.cuda.current_device())
     if engine == "tensor":
         c.tune(0)   # kernel, time splits and grid chosen by timing
-    # A dedicated stream: the engine launches and the timing events share it.
-    stream = torch.cuda.Stream()
-    c.set_stream(stream.cuda_stream)
+    # The timing events go on the context's own stream, where consecutive
+    # accumulating calls may overlap (programmatic dependent launch).
+    stream = torch.cuda.ExternalStream(c.stream)
     nbytes = int(c.info.vecLength) * 2
     nbuf = max(1, min(max_bufs, -(-min_rotate_bytes // nbytes)))
     bufs = []

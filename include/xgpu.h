@@ -86,7 +86,7 @@ typedef struct XGPUInfoStruct {
   long long unsigned int triLength;      /* Complex elements in triangular order */
   unsigned int matrix_order;  /* one of the *_ORDER codes */
   size_t shared_atomic_size;  /* kept for layout compatibility; reports 4 */
-  size_t complex_block_size;  /* kept for layout compatibility; reports 1 */
+  size_t complex_block_size;  /* 32 for an XGPU_INPUT_BLOCK32 context, else 1 */
 } XGPUInfo;
 
 /* Caller-owned context (xgpu.h:94-113), byte-identical to xGPU's. */
@@ -216,6 +216,9 @@ void xgpuOmpXengine(Complex *matrix_h, ComplexInput *array_h);
 #define XGPU_INPUT_PACKED4  1  /* [t][f][s][p] one byte: re in the high nibble,
                                   im in the low nibble, 4-bit two's complement */
 #define XGPU_INPUT_DP4A_SWIZZLED 2 /* xgpuSwizzleInput's [t/4][f][s][p][c][t%4] */
+#define XGPU_INPUT_BLOCK32  3  /* xGPU built with COMPLEX_BLOCK_SIZE=32: per 16
+                                  stations, 32 bytes of {X.re,Y.re} pairs then
+                                  32 bytes of {X.im,Y.im} pairs */
 
 typedef struct XGPUConfigStruct {
   unsigned int nstation;     /* multiple of 16 */
@@ -265,6 +268,14 @@ int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long 
  * NULL returns to the context's own stream.  The caller keeps the stream alive
  * until xgpuFree or the next xgpuSetComputeStream. */
 int xgpuSetComputeStream(XGPUContext *context, void *stream);
+
+/* The stream (a cudaStream_t) the context queues its device work on: its own
+ * unless xgpuSetComputeStream chose another; NULL for an uninitialised
+ * context.  On its own stream a context lets an accumulating call over
+ * device-resident input start while the previous call's launch finishes (the
+ * two only add into the integration), so callers that time or order work
+ * should record their events on this stream rather than switch streams. */
+void *xgpuComputeStream(XGPUContext *context);
 
 /* Extension with no counterpart in the reference: correlate once without
  * allocating anything, for callers that cannot call cudaMalloc where they

@@ -64,6 +64,7 @@ def lib():
                                       ctypes.c_double]
         L.oracle_generate_range.argtypes = [c_i8p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint64,
                                             ctypes.c_double, ctypes.c_uint64]
+        L.oracle_block32_input.argtypes = [c_i8p, ctypes.c_size_t, c_i8p]
         L.oracle_unpack4.argtypes = [ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t, c_i8p]
         L.oracle_num_threads.restype = ctypes.c_int
         _lib = L
@@ -162,6 +163,15 @@ def reorder(matrix_words, n, f, order):
     u = m.view(np.uint32)
     lib().oracle_reorder_matrix(_p(u, ctypes.c_uint32), n, f, order)
     return m
+
+
+def block32(inp):
+    """Standard input -> xGPU's COMPLEX_BLOCK_SIZE=32 layout (omp_xengine.c:61-78)."""
+    inp = np.ascontiguousarray(inp, dtype=np.int8)
+    assert inp.size % 64 == 0
+    out = np.empty_like(inp)
+    lib().oracle_block32_input(_p(inp, ctypes.c_int8), inp.size, _p(out, ctypes.c_int8))
+    return out
 
 
 def swizzle(inp, n, f, t):

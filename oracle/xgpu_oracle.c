@@ -192,6 +192,21 @@ void oracle_swizzle_input(const int8_t *in, int N, int F, int T, int8_t *out) {
                 in[((((size_t)t * F + f) * N + s) * NPOL + p) * 2 + c];
 }
 
+/* [t][f][s][p]{re,im} -> xGPU's COMPLEX_BLOCK_SIZE=32 layout, the inverse of
+ * the reader in omp_xengine.c:61-78.  The flat (t,f,s) station index g falls
+ * in 64-byte block g/16 at slot k = g%16: bytes 2k, 2k+1 hold the real parts
+ * of polarisations X, Y and bytes 32+2k, 33+2k their imaginary parts.
+ * nbytes = 4*T*F*N, a multiple of 64. */
+void oracle_block32_input(const int8_t *in, size_t nbytes, int8_t *out) {
+  for (size_t g = 0; g < nbytes / 4; g++) {
+    int8_t *b = out + 64 * (g / 16) + 2 * (g % 16);
+    b[0] = in[4 * g + 0];
+    b[1] = in[4 * g + 2];
+    b[32] = in[4 * g + 1];
+    b[33] = in[4 * g + 3];
+  }
+}
+
 /* Triangular -> full Hermitian [f][i][j][p1][p2] for float re/im pairs
  * (cpu_util.c:258-279). */
 void oracle_extract_matrix_f32(const float *packed, int N, int F, float *full) {

@@ -79,6 +79,10 @@ def main():
                 m = oracle.tri_to_order(words, n, f, order)
                 arrays[f"{shape}_{var}_matrix"] = m
                 arrays[f"{shape}_{var}_reordered"] = R.reorder(m)[: words.size]
+            # The reference's COMPLEX_BLOCK_SIZE=32 reader on the oracle's
+            # blocked copy of the same input.
+            arrays[f"{shape}_omp_dp4a_b32"] = oracle.RefLib(shape, "dp4a_rt_b32").omp_xengine(
+                oracle.block32(x))
             R = oracle.RefLib(shape, "fp32_rt")
             arrays[f"{shape}_swizzled"] = R.swizzle(x)
             arrays[f"{shape}_extract_fp32"] = R.extract(ref_flt)

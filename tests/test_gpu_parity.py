@@ -178,6 +178,27 @@ def test_dp4a_swizzled_input(xg, oracle_mod, engine):
     assert np.array_equal(ex, oracle_mod.xengine_i64(x, n, f, t))
 
 
+@pytest.mark.parametrize("engine,compute", [("tensor", "int8"), ("plain", "int8"),
+                                            ("plain", "fp32")])
+def test_block32_input(xg, oracle_mod, engine, compute):
+    """xGPU's COMPLEX_BLOCK_SIZE=32 input layout, unblocked on the device."""
+    n, f, t = 48, 3, 512
+    x = oracle_mod.gaussian_input(n, f, t, seed=21, sigma=40.0)
+    out = "int32" if compute == "int8" else "float32"
+    with xg.Correlator(n, f, t, engine=engine, compute=compute, output=out,
+                       input_format="block32") as c:
+        assert c.info.complex_block_size == 32
+        c.set_input(oracle_mod.block32(x))
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2]
+        exact = oracle_mod.xengine_i64(x, n, f, t)
+        if compute == "int8":
+            assert np.array_equal(c.dump_int64(), exact)
+            assert np.array_equal(got, exact.astype(np.int32))
+        else:
+            assert np.array_equal(got, oracle_mod.xengine_f32(x, n, f, t))
+
+
 def test_device_generator_matches_host(xg, oracle_mod):
     import torch
     for kind, sigma in [(0, 16.0), (0, 40.0), (1, 0.0), (2, 0.0)]:
@@ -263,7 +284,7 @@ def test_reference_api_default_context(xg, oracle_mod):
     L.xgpuFree(ctypes.byref(ctx))
 
 
-@pytest.mark.parametrize("fmt", ["packed4", "dp4a_swizzled"])
+@pytest.mark.parametrize("fmt", ["packed4", "dp4a_swizzled", "block32"])
 def test_converted_inputs_back_to_back(xg, oracle_mod, fmt):
     """Several calls in flight: each call's input conversion runs on its own
     stream into one of two buffers, under the previous call's correlation."""
@@ -277,7 +298,8 @@ def test_converted_inputs_back_to_back(xg, oracle_mod, fmt):
         else:
             x = oracle_mod.gaussian_input(n, f, t, seed=50 + s)
             raws.append(x)
-            feeds.append(oracle_mod.swizzle(x, n, f, t))
+            feeds.append(oracle_mod.swizzle(x, n, f, t) if fmt == "dp4a_swizzled"
+                         else oracle_mod.block32(x))
     with xg.Correlator(n, f, t, engine="tensor", input_format=fmt) as c:
         for q, feed in enumerate(feeds):
             c.set_input(feed)
@@ -301,3 +323,46 @@ def test_converted_device_input_on_caller_stream(xg, oracle_mod):
                 stream.synchronize()
             oracle_mod.xengine_i64(oracle_mod.unpack4(p), n, f, t, acc=want)
         assert np.array_equal(c.dump_int64(), want)
+
+
+@pytest.mark.parametrize("pair,ksplit", [(0, 1), (1, 1), (0, 3), (2, 1)])
+def test_overlapping_accumulating_calls(xg, oracle_mod, pair, ksplit):
+    """Back-to-back accumulating calls over device input on the context's own
+    stream: each launch may start before the previous one has finished (the
+    two only add into the integration).  Sums stay exact, also across a dump
+    in the middle and a clear."""
+    import torch
+    n, f, t = 128, 5, 1024
+    xs = [oracle_mod.gaussian_input(n, f, t, seed=90 + q, sigma=30.0) for q in range(5)]
+    ds = [torch.from_numpy(x).cuda() for x in xs]
+    torch.cuda.synchronize()
+    one = sum(oracle_mod.xengine_i64(x, n, f, t) for x in xs)
+    with xg.Correlator(n, f, t, engine="tensor") as c:
+        c.tune(ksplit, 0, pair)
+        for _ in range(3):
+            for d in ds:
+                c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        assert np.array_equal(c.dump_int64(), 3 * one)
+        for d in ds:
+            c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        assert np.array_equal(c.dump_int64(), 4 * one)
+        c.clear()
+        for d in ds[::-1]:
+            c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        c.run_device(ds[0].data_ptr(), xg.SYNCOP_SYNC_COMPUTE)
+        assert np.array_equal(c.dump_int64(), one + oracle_mod.xengine_i64(xs[0], n, f, t))
+
+
+def test_overlapping_calls_of_several_segments(xg, oracle_mod):
+    """Calls longer than one launch (several time segments) chained back to back."""
+    import torch
+    n, f, t = 32, 2, 65536 + 512
+    xs = [oracle_mod.gaussian_input(n, f, t, seed=70 + q, sigma=20.0) for q in range(2)]
+    ds = [torch.from_numpy(x).cuda() for x in xs]
+    torch.cuda.synchronize()
+    with xg.Correlator(n, f, t, ntimepipe=128, engine="tensor") as c:
+        for d in ds + ds:
+            c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        got = c.dump_int64()
+    want = 2 * sum(oracle_mod.xengine_i64(x, n, f, t) for x in xs)
+    assert np.array_equal(got, want)

@@ -85,6 +85,24 @@ def test_swizzle_and_extract(oracle_mod, golden, shape):
                           arr[f"{shape}_extract_fp32"])
 
 
+@pytest.mark.parametrize("shape", ["s16", "s32"])
+def test_block32_layout_matches_reference_reader(oracle_mod, golden, shape):
+    """The reference built with COMPLEX_BLOCK_SIZE=32 (its reader,
+    omp_xengine.c:61-78) sees the oracle's blocked copy of an input as the
+    same samples: its output equals the standard build's on the plain input."""
+    _, arr = golden
+    n, f, t, _ = oracle_mod.REF_SHAPES[shape]
+    x = arr[f"{shape}_input"]
+    assert np.array_equal(arr[f"{shape}_omp_dp4a_b32"], arr[f"{shape}_omp_dp4a"])
+    assert np.array_equal(oracle_mod.xengine_i64(x, n, f, t),
+                          arr[f"{shape}_omp_dp4a_b32"].astype(np.int64))
+    b = oracle_mod.block32(x)
+    assert np.array_equal(np.sort(b), np.sort(x))      # a permutation of the bytes
+    if oracle_mod.ref_available(shape, "dp4a_rt_b32"):
+        ref = oracle_mod.RefLib(shape, "dp4a_rt_b32").omp_xengine(b)
+        assert np.array_equal(ref, arr[f"{shape}_omp_dp4a"])
+
+
 def test_oracle_accumulates(oracle_mod):
     n, f, t = 16, 2, 64
     a = oracle_mod.gaussian_input(n, f, t, seed=3)

@@ -35,7 +35,7 @@ XGPU_HOST_BUFFER_NOT_SET = 5
 XGPU_INVALID_ARGUMENT = 6
 SYNCOP_NONE, SYNCOP_DUMP, SYNCOP_SYNC_TRANSFER, SYNCOP_SYNC_COMPUTE = 0, 1, 2, 3
 XGPU_ENGINE_DEFAULT, XGPU_ENGINE_PLAIN, XGPU_ENGINE_TENSOR = 0, 1, 2
-XGPU_INPUT_INT8, XGPU_INPUT_PACKED4, XGPU_INPUT_DP4A_SWIZZLED = 0, 1, 2
+XGPU_INPUT_INT8, XGPU_INPUT_PACKED4, XGPU_INPUT_DP4A_SWIZZLED, XGPU_INPUT_BLOCK32 = 0, 1, 2, 3
 
 ERROR_NAMES = {
     XGPU_OK: "XGPU_OK",
@@ -148,6 +148,7 @@ _PROTOTYPES = [
     ("xgpuGenerateDevice", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
                                           ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int]),
     ("xgpuSetComputeStream", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_void_p]),
+    ("xgpuComputeStream", ctypes.c_void_p, [ctypes.POINTER(XGPUContext)]),
     ("xgpuEngineName", ctypes.c_char_p, [ctypes.POINTER(XGPUContext)]),
     ("xgpuCorrelateStatic", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(XGPUConfig), ctypes.c_int,
@@ -226,7 +227,7 @@ ENGINES = {"default": XGPU_ENGINE_DEFAULT, "plain": XGPU_ENGINE_PLAIN, "tensor":
 ORDERS = {"tri": TRIANGULAR_ORDER, "ri": REAL_IMAG_TRIANGULAR_ORDER,
           "rt": REGISTER_TILE_TRIANGULAR_ORDER}
 FORMATS = {"int8": XGPU_INPUT_INT8, "packed4": XGPU_INPUT_PACKED4,
-           "dp4a_swizzled": XGPU_INPUT_DP4A_SWIZZLED}
+           "dp4a_swizzled": XGPU_INPUT_DP4A_SWIZZLED, "block32": XGPU_INPUT_BLOCK32}
 
 
 class Correlator:
@@ -311,6 +312,12 @@ class Correlator:
         return check("xgpuSetComputeStream",
                      lib().xgpuSetComputeStream(ctypes.byref(self.ctx),
                                                 ctypes.c_void_p(stream_handle)))
+
+    @property
+    def stream(self):
+        """Handle (cudaStream_t as int) of the stream the context queues work on;
+        wrap it with torch.cuda.ExternalStream to record events on it."""
+        return lib().xgpuComputeStream(ctypes.byref(self.ctx)) or 0
 
     def close(self):
         if self.ctx.internal:

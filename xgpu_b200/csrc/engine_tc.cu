@@ -70,6 +70,7 @@ struct Params {
   int *err;
   int stall;           // test switch: issue no loads (the waits on them expire)
   int streamk;         // single job: each CTA takes an equal share of all (tile, stage) steps
+  int overlap;         // may run alongside the previous (accumulating) launch of the stream
 };
 
 // A decoded work item.  The scheduler decodes each item once and publishes it
@@ -85,21 +86,9 @@ struct Item {
   const CUtensorMap *map;
 };
 
-__device__ __forceinline__ Item decode_item(const Params &p, int u) {
+__device__ __forceinline__ Item decode_job(const Job &j, int u) {
   Item it;
   it.u = u;
-  const Job *jp;
-  if (p.jobs) {
-    int lo = 0, hi = p.njobs - 1;   // last job with item_begin <= u
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (p.jobs[mid].item_begin <= u) lo = mid; else hi = mid - 1;
-    }
-    jp = &p.jobs[lo];
-  } else {
-    jp = &p.single;
-  }
-  const Job &j = *jp;
   const int v = u - j.item_begin;
   const int k = v % j.npairs;          // tile within the channel
   const int rest = v / j.npairs;
@@ -121,6 +110,20 @@ __device__ __forceinline__ Item decode_item(const Params &p, int u) {
   it.state = j.state;
   it.map = &j.map;
   return it;
+}
+
+__device__ __forceinline__ Item decode_item(const Params &p, int u) {
+  if (p.jobs) {
+    int lo = 0, hi = p.njobs - 1;   // last job with item_begin <= u
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.jobs[mid].item_begin <= u) lo = mid; else hi = mid - 1;
+    }
+    return decode_job(p.jobs[lo], u);
+  }
+  // Named parameter fields: constant-bank reads rather than generic loads
+  // through a pointer that may point to either space.
+  return decode_job(p.single, u);
 }
 
 // Bytes of station row il (0..31) of the item's tile inside the integration
@@ -186,6 +189,15 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t stage0 = smem_u32(smem);
+  // Prologue done.  Unless this launch only adds into sums that the previous
+  // launch of the stream (an engine launch of the same context) also only
+  // adds into, nothing below touches global memory before the previous launch
+  // has finished; an overlapping launch waits for it at the end instead, so it
+  // never completes first.  The next launch may start once this one has
+  // waited: a chain of overlapping launches thus only ever runs beside
+  // launches that add, never beside a store or anything else queued earlier.
+  if (!p.overlap) pdl_wait();
+  pdl_trigger();
 
   auto fail = [&](int code) {
     atomicExch(p.err, code);
@@ -342,23 +354,21 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       if (jmax > kStations) jmax = kStations;
       if (t.tr == t.tc && il + 1 < jmax) jmax = il + 1;
       if (t.tr * kStations + il >= t.n) jmax = 0;
-#pragma unroll 1
+      uint32_t v[kTile / 32][32];
+      tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kTile), v);
+      // Accumulator fully read: the MMA warp may reuse it.
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty0 + 8 * acc);
+#pragma unroll
       for (int q = 0; q < kTile / 32; ++q) {
-        uint32_t v[32];
-        tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kTile + q * 32), v);
-        if (q == kTile / 32 - 1) {
-          // Accumulator fully read: the MMA warp may reuse it.
-          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-          __syncwarp();
-          if (lane == 0) mbar_arrive(tempty0 + 8 * acc);
-        }
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
           // Columns 4jj..4jj+3: (p2=0 re, p2=0 im, p2=1 re, p2=1 im) of station
           // j.  The real-row lane produces p2 = 0, the imaginary-row lane p2 = 1;
           // each needs two values from its partner lane.
-          const int v0 = (int)v[4 * jj], v1 = (int)v[4 * jj + 1];
-          const int v2 = (int)v[4 * jj + 2], v3 = (int)v[4 * jj + 3];
+          const int v0 = (int)v[q][4 * jj], v1 = (int)v[q][4 * jj + 1];
+          const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
           const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
           const int rb = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
           const long long re = c ? (long long)ra + v3 : (long long)v0 + rb;
@@ -383,6 +393,8 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
     if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 
+  __syncwarp();   // lanes 1-31 of the producer and MMA warps wait for lane 0
+  if (p.overlap) pdl_wait();
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 1) {
@@ -468,13 +480,13 @@ int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                       int overwrite, int *err, cudaStream_t st) {
   TcTuning tune;   // single CTAs, no time split, one CTA per SM
-  return launch_tc_tuned(map, s, t0, tcount, state, overwrite, err, st, tune);
+  return launch_tc_tuned(map, s, t0, tcount, state, overwrite, err, st, tune, 0);
 }
 
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune) {
-  if (tune.wide) return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune);
+                            const TcTuning &tune, int overlap) {
+  if (tune.wide) return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap);
   const int sms = tc_num_sms();
   if (!sms) return cudaErrorInvalidDevice;
   static bool configured = false;
@@ -521,10 +533,22 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
   p.stall = tune.stall;
   // Stream-K only when every piece adds into existing sums (no stores).
   p.streamk = (tune.streamk && !j.store && ksplit == 1) ? 1 : 0;
+  p.overlap = (overlap && !overwrite) ? 1 : 0;
   int grid = tune.grid > 0 ? tune.grid : sms;
   if (grid > p.total) grid = p.total;
-  tc::xengine_tc_kernel<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(p);
-  return cudaGetLastError();
+  // Programmatic launch: this grid's prologue overlaps the previous kernel's
+  // tail (the kernel waits for it before touching global memory).
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(tc::kThreads);
+  cfg.dynamicSmemBytes = tc::kSmemBytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, tc::xengine_tc_kernel, p);
 }
 
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -547,6 +571,7 @@ cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int
   p.err = err;
   p.stall = 0;
   p.streamk = 0;
+  p.overlap = 0;
   if (grid <= 0) grid = sms;
   if (grid > total_items) grid = total_items;
   if (grid < 1) return cudaSuccess;

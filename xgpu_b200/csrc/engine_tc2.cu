@@ -57,6 +57,7 @@ struct Params {
   int *queue;          // dynamic work counter (zeroed before launch); nullptr: static stride
   int *err;
   int stall;           // test switch: issue no loads (the waits on them expire)
+  int overlap;         // may run alongside the previous (accumulating) launch of the stream
 };
 
 // A decoded work item, 64 bytes; the leader's scheduler writes it into both
@@ -72,17 +73,23 @@ struct Item {
 };
 static_assert(sizeof(Item) == 64, "ring entries are copied as 8 words");
 
+__device__ __forceinline__ Item decode_job(const Job &j, int u);
+
 __device__ __forceinline__ Item decode(const Params &p, int u) {
-  const Job *jp = &p.job;
   if (p.jobs) {
     int lo = 0, hi = p.njobs - 1;   // last job with item_begin <= u
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (p.jobs[mid].item_begin <= u) lo = mid; else hi = mid - 1;
     }
-    jp = &p.jobs[lo];
+    return decode_job(p.jobs[lo], u);
   }
-  const Job &j = *jp;
+  // Named parameter fields: constant-bank reads rather than generic loads
+  // through a pointer that may point to either space.
+  return decode_job(p.job, u);
+}
+
+__device__ __forceinline__ Item decode_job(const Job &j, int u) {
   Item it;
   it.u = u;
   const int v = u - j.item_begin;
@@ -247,6 +254,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t stage0 = smem_u32(smem);
+  // Prologue done.  Unless this launch only adds into sums that the previous
+  // launch of the stream (an engine launch of the same context) also only
+  // adds into, nothing below touches global memory before the previous launch
+  // has finished; an overlapping launch waits for it at the end instead, so it
+  // never completes first.  The next launch may start once this one has
+  // waited: a chain of overlapping launches thus only ever runs beside
+  // launches that add, never beside a store or anything else queued earlier.
+  if (!p.overlap) pdl_wait();
+  pdl_trigger();
 
   auto fail = [&](int code) {
     atomicExch(p.err, code);
@@ -408,16 +424,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         if (jmax > kStations) jmax = kStations;
         if (cb == rb && il + 1 < jmax) jmax = il + 1;
         if (i_glob >= t.n) jmax = 0;
-#pragma unroll 1
+        uint32_t v[kHalf / 32][32];
+        tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccCols + h * kHalf),
+                   v);
+#pragma unroll
         for (int q = 0; q < kHalf / 32; ++q) {
-          uint32_t v[32];
-          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) +
-                        (uint32_t)(acc * kAccCols + h * kHalf + q * 32),
-                    v);
 #pragma unroll
           for (int jj = 0; jj < 8; ++jj) {
-            const int v0 = (int)v[4 * jj], v1 = (int)v[4 * jj + 1];
-            const int v2 = (int)v[4 * jj + 2], v3 = (int)v[4 * jj + 3];
+            const int v0 = (int)v[q][4 * jj], v1 = (int)v[q][4 * jj + 1];
+            const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
             const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
             const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
             const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
@@ -453,6 +468,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 
+  __syncwarp();   // lanes 1-31 of the producer and MMA warps wait for lane 0
+  if (p.overlap) pdl_wait();
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   cluster_sync();
@@ -467,7 +484,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 }  // namespace tc2
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
-                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune) {
+                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap) {
   static int num_sms = 0;
   static bool configured = false;
   if (!configured) {
@@ -512,11 +529,23 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   p.total = j.items;
   p.err = err;
   p.stall = tune.stall;
+  p.overlap = (overlap && !overwrite) ? 1 : 0;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
   if (clusters > p.total) clusters = p.total;
   if (clusters < 1) clusters = 1;
-  tc2::xengine_tc2_kernel<<<2 * clusters, tc2::kThreads, tc2::kSmemBytes, st>>>(p);
-  return cudaGetLastError();
+  // Programmatic launch: this grid's prologue overlaps the previous kernel's
+  // tail (the kernel waits for it before touching global memory).
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(2 * clusters));
+  cfg.blockDim = dim3(tc2::kThreads);
+  cfg.dynamicSmemBytes = tc2::kSmemBytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, tc2::xengine_tc2_kernel, p);
 }
 
 cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -540,6 +569,7 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
   p.queue = queue;
   p.err = err;
   p.stall = 0;
+  p.overlap = 0;
   int clusters = (grid > 0 ? grid : sms) / 2;
   if (clusters > total_items) clusters = total_items;
   if (clusters < 1) return cudaSuccess;

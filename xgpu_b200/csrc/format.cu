@@ -103,6 +103,26 @@ __global__ void unswizzle_kernel(const uint32_t *in, int8_t *out, long long grou
   }
 }
 
+// xGPU's COMPLEX_BLOCK_SIZE=32 input (read by omp_xengine.c:61-78,
+// shared_transfer_4.cuh:69-86) -> [t][f][s][p]{re,im}.  A 64-byte block holds
+// 16 consecutive (t,f,s) stations: {X.re,Y.re} pairs in bytes 0-31, {X.im,Y.im}
+// pairs in bytes 32-63.  One thread turns 4 stations (8 + 8 bytes) into 16.
+__global__ void unblock32_kernel(const uint2 *in, uint4 *out, long long quads) {
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < quads;
+       u += (long long)gridDim.x * blockDim.x) {
+    const long long blk = u >> 2;
+    const int q = (int)(u & 3);
+    const uint2 re = in[blk * 8 + q];      // bytes 8q .. 8q+7 of the block
+    const uint2 im = in[blk * 8 + 4 + q];  // bytes 32+8q ..
+    uint4 o;
+    o.x = __byte_perm(re.x, im.x, 0x5140);
+    o.y = __byte_perm(re.x, im.x, 0x7362);
+    o.z = __byte_perm(re.y, im.y, 0x5140);
+    o.w = __byte_perm(re.y, im.y, 0x7362);
+    out[u] = o;
+  }
+}
+
 // Seeded synthetic bytes; the same hash and tables as the host generator.
 struct GenParams {
   uint32_t thr[254];
@@ -190,6 +210,13 @@ cudaError_t launch_unswizzle_dp4a(const int8_t *in, int8_t *out, const Sizes &s,
   const long long groups = (long long)(s.t / 4) * row_bytes;
   fmt::unswizzle_kernel<<<fmt::grid_for(groups, 256), 256, 0, st>>>((const uint32_t *)in, out,
                                                                     groups, row_bytes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unblock32(const int8_t *in, int8_t *out, long long nbytes, cudaStream_t st) {
+  const long long quads = nbytes / 16;
+  fmt::unblock32_kernel<<<fmt::grid_for(quads, 256), 256, 0, st>>>((const uint2 *)in,
+                                                                   (uint4 *)out, quads);
   return cudaGetLastError();
 }
 

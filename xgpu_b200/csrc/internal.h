@@ -56,12 +56,19 @@ cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcou
 // Tensor-core engine.  The tensor map describes `in` (see make_tc_tensor_map).
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                       int64_t *state, int overwrite, int *err, cudaStream_t st);
+// Launched programmatically (PDL): the prologue overlaps the previous kernel of
+// the stream.  overlap = 1 promises that the previous kernel of the stream is
+// an engine launch of the same integration that does not store (only adds)
+// and that nothing this launch reads was written after it was queued: then,
+// unless this launch stores, the two run side by side, their reduce-adds
+// commuting.
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune);
+                            const TcTuning &tune, int overlap);
 // The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
-                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune);
+                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune,
+                       int overlap);
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -83,6 +90,7 @@ cudaError_t tc_check_device();
 // ---- input conversion, output formatting, synthetic input -----------------
 cudaError_t launch_unpack4(const uint8_t *in, int8_t *out, long long nsamples, cudaStream_t st);
 cudaError_t launch_unswizzle_dp4a(const int8_t *in, int8_t *out, const Sizes &s, cudaStream_t st);
+cudaError_t launch_unblock32(const int8_t *in, int8_t *out, long long nbytes, cudaStream_t st);
 // state (int64 or float) -> Complex words in `order` of type out_type.
 cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s, int order,
                           int out_type, void *out, cudaStream_t st);

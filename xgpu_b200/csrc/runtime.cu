@@ -85,6 +85,10 @@ struct Internal {
   int cur = 0;
   bool state_zero = true;
   TcTuning tune;   // tensor-core kernel, time splits and grid
+  // The last operation queued on s_comp is an engine launch that only added
+  // into the integration buffer (no store), on the context's own stream: the
+  // next accumulating launch over other input may overlap it.
+  bool adding_tail = false;
 
   // tensor maps, cached by device pointer
   struct MapEntry {
@@ -138,7 +142,7 @@ int validate(const XGPUConfig &c) {
     return 0;
   if (c.engine > XGPU_ENGINE_TENSOR) return 0;
   if (c.engine == XGPU_ENGINE_TENSOR && c.compute_type != XGPU_INT8) return 0;
-  if (c.input_format > XGPU_INPUT_DP4A_SWIZZLED) return 0;
+  if (c.input_format > XGPU_INPUT_BLOCK32) return 0;
   // input bytes of one call must fit the 32-bit sample index space of the engines
   const double bytes = 4.0 * c.nstation * c.nfrequency * (double)c.ntime;
   if (bytes > 1.0e12) return 0;
@@ -160,7 +164,7 @@ void fill_info(const XGPUConfig &c, const Sizes &s, XGPUInfo *info) {
   info->triLength = (unsigned long long)s.tri_length;
   info->matrix_order = c.matrix_order;
   info->shared_atomic_size = 4;
-  info->complex_block_size = 1;
+  info->complex_block_size = c.input_format == XGPU_INPUT_BLOCK32 ? 32 : 1;
 }
 
 int free_device(Internal *in) {
@@ -233,6 +237,12 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   const Sizes &s = in->sz;
   const int8_t *x = (const int8_t *)d_input;
   int conv = -1;
+  // Overlap with the previous launch only when nothing else sits between them
+  // on the stream (no conversion, no copy to wait for) and that launch only
+  // added into the buffer.
+  bool tail = in->adding_tail && in->s_comp == in->s_own && !input_ready &&
+              in->cfg.input_format == XGPU_INPUT_INT8;
+  in->adding_tail = false;
   if (in->cfg.input_format != XGPU_INPUT_INT8) {
     conv = in->conv_cur;
     in->conv_cur ^= 1;
@@ -245,6 +255,9 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
     }
     if (in->cfg.input_format == XGPU_INPUT_PACKED4)
       XGPU_CHECK(launch_unpack4((const uint8_t *)d_input, in->d_conv[conv], s.vec_length, in->s_conv));
+    else if (in->cfg.input_format == XGPU_INPUT_BLOCK32)
+      XGPU_CHECK(launch_unblock32((const int8_t *)d_input, in->d_conv[conv], 2 * s.vec_length,
+                                  in->s_conv));
     else
       XGPU_CHECK(launch_unswizzle_dp4a((const int8_t *)d_input, in->d_conv[conv], s, in->s_conv));
     XGPU_CHECK(cudaEventRecord(in->conv_done[conv], in->s_conv));
@@ -270,9 +283,12 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
     }
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
-                                 in->d_err, in->s_comp, in->tune));
+      const int store = ow && t0 == 0;
+      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
+                                 in->s_comp, in->tune, tail && !store ? 1 : 0));
+      tail = !store;   // the next segment follows an adding launch
     }
+    in->adding_tail = tail && conv < 0;
   }
   in->state_zero = false;
   if (conv >= 0) {
@@ -284,6 +300,7 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
 
 // Read and clear the device error word; s_comp must be idle.
 int check_device_error(Internal *in) {
+  in->adding_tail = false;
   XGPU_CHECK(cudaMemcpyAsync(in->h_err, in->d_err, sizeof(int), cudaMemcpyDeviceToHost,
                              in->s_comp));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
@@ -298,6 +315,7 @@ int check_device_error(Internal *in) {
 }
 
 int dump(XGPUContext *ctx, Internal *in) {
+  in->adding_tail = false;
   if (!in->matrix_h_set || !ctx->matrix_h) return XGPU_HOST_BUFFER_NOT_SET;
   if (ctx->matrix_len && ctx->output_offset + (size_t)in->sz.mat_length > ctx->matrix_len)
     return XGPU_INVALID_ARGUMENT;
@@ -601,6 +619,7 @@ int xgpuCudaXengine(XGPUContext *context, int syncOp) {
   int r = run_engine(in, in->d_in[b], in->copy_done[b]);
   if (r != XGPU_OK) return r;
   XGPU_CHECK(cudaEventRecord(in->comp_done[b], in->s_comp));
+  in->adding_tail = false;
   return finish_call(context, in, syncOp);
 }
 
@@ -627,6 +646,7 @@ int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_o
   if (!in) return XGPU_NOT_INITIALIZED;
   if (!host_out || !in->int_state) return XGPU_INVALID_ARGUMENT;
   XGPU_CHECK(cudaSetDevice(in->device));
+  in->adding_tail = false;
   const size_t bytes = (size_t)in->sz.state_elems * 8;
   if (in->state_zero) {
     XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
@@ -644,6 +664,7 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream) {
   XGPU_CHECK(cudaSetDevice(in->device));
   cudaStream_t next = stream ? (cudaStream_t)stream : in->s_own;
   if (next == in->s_comp) return XGPU_OK;
+  in->adding_tail = false;
   // Order the new stream after everything queued on the old one.
   cudaEvent_t ev;
   XGPU_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -654,10 +675,16 @@ int xgpuSetComputeStream(XGPUContext *context, void *stream) {
   return XGPU_OK;
 }
 
+void *xgpuComputeStream(XGPUContext *context) {
+  Internal *in = get(context);
+  return in ? (void *)in->s_comp : nullptr;
+}
+
 int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   Internal *in = get(context);
   if (!in) return XGPU_NOT_INITIALIZED;
   if (ksplit < 0 || grid < 0 || pair < 0 || pair > 2) return XGPU_INVALID_ARGUMENT;
+  in->adding_tail = false;
   if (ksplit > 0) {
     in->tune.ksplit = ksplit;
     in->tune.grid = grid;
@@ -699,7 +726,7 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
     auto run = [&]() {
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-        if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t) !=
+        if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t, 0) !=
             cudaSuccess)
           return false;
       }

@@ -120,7 +120,9 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// tcgen05.ld of 32 columns x 32 lanes (one register per column) without the
+// wait; tmem_ld_wait below completes it.
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
       "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -131,8 +133,51 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
         "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
+}
+
+// Ties the registers of an earlier tmem_ld32_async to a point after
+// tcgen05.wait::ld, so the compiler cannot move their uses above the wait.
+__device__ __forceinline__ void tmem_regs_after_wait(uint32_t (&v)[32]) {
+  asm volatile(""
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
+                 "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]),
+                 "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]),
+                 "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]),
+                 "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]),
+                 "+r"(v[30]), "+r"(v[31])
+               :
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+
+// Four 32-column loads in flight, one wait: 128 columns of this warp's lanes.
+__device__ __forceinline__ void tmem_ld128(uint32_t taddr, uint32_t (&v)[4][32]) {
+  tmem_ld32_async(taddr, v[0]);
+  tmem_ld32_async(taddr + 32, v[1]);
+  tmem_ld32_async(taddr + 64, v[2]);
+  tmem_ld32_async(taddr + 96, v[3]);
+  tmem_ld_wait();
+  tmem_regs_after_wait(v[0]);
+  tmem_regs_after_wait(v[1]);
+  tmem_regs_after_wait(v[2]);
+  tmem_regs_after_wait(v[3]);
+}
+
+// Programmatic dependent launch.  pdl_trigger lets the next kernel of the
+// stream start its prologue now; pdl_wait blocks until the previous kernel of
+// the stream (when this one was launched programmatically) has completed and
+// its memory is visible.  Both are no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 
 constexpr int kEpiThreads = 128;   // four epilogue warps, one per TMEM lane quarter
 

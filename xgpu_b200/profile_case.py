@@ -2,6 +2,7 @@
 
     python -m xgpu_b200.profile_case --n 512 --f 32 --t 8192 [--engine tensor|plain|fp32]
                                      [--reps 5] [--warmup 3] [--ksplit K] [--accumulate]
+                                     [--caller-stream]
 
 Prints one JSON line: milliseconds per xgpuCudaXengineDevice call (CUDA
 events on the engine's stream), X-engine TOPS (16*F*T*N(N+1) ops per call)
@@ -29,6 +30,8 @@ def main():
     ap.add_argument("--accumulate", action="store_true",
                     help="add into the integration (default: every call starts a new one)")
     ap.add_argument("--sigma", type=float, default=16.0)
+    ap.add_argument("--caller-stream", action="store_true",
+                    help="run on a caller stream (xgpuSetComputeStream) instead of the context's")
     args = ap.parse_args()
 
     import torch
@@ -38,8 +41,11 @@ def main():
                       output="int32" if compute == "int8" else "float32", order="tri")
     if args.ksplit >= 0 or args.pair:
         c.tune(max(args.ksplit, 0) if args.ksplit != -1 else 1, 0, args.pair)
-    stream = torch.cuda.Stream()
-    c.set_stream(stream.cuda_stream)
+    if args.caller_stream:
+        stream = torch.cuda.Stream()
+        c.set_stream(stream.cuda_stream)
+    else:
+        stream = torch.cuda.ExternalStream(c.stream)
     nbytes = int(c.info.vecLength) * 2
     x = torch.empty(nbytes, dtype=torch.int8, device="cuda")
     xg.generate_device(x.data_ptr(), nbytes, 0, 7, args.sigma, torch.cuda.current_device())
