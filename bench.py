@@ -146,6 +146,9 @@ def max_over_ranks(world, value):
     return float(t.item())
 
 
+TUNING = {}   # (engine, n, f, t) -> the tensor engine's autotuned setting
+
+
 def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, seed=1,
                      sigma=SIGMA, min_rotate_bytes=2 * L2_BYTES, max_bufs=16):
     """Average ms per xgpuCudaXengineDevice call (input resident in HBM).  The
@@ -178,6 +181,7 @@ def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, 
     torch.cuda.synchronize()
     barrier(world)
     ms = e0.elapsed_time(e1) / steps
+    TUNING[(engine, n, f, t)] = c.tuning() if engine == "tensor" else None
     c.close()
     del bufs
     torch.cuda.empty_cache()
@@ -547,7 +551,10 @@ def main():
                                "integration buffer",
                    "nstation": N, "npol": 2, "nfrequency": F, "ntime": T,
                    "parallelism": f"channel-sharded replicas x{world} (no collective)",
-                   "l2": f"input rotates over {rot_bytes / 2**20:.0f} MiB of buffers (> 126 MiB L2)"},
+                   "l2": f"input rotates over {rot_bytes / 2**20:.0f} MiB of buffers (> 126 MiB L2)",
+                   "tuning": TUNING.get(("tensor", N, F, T)),
+                   "launches": "programmatic (PDL): each accumulating call may start while the "
+                               "previous call's launch finishes; ms_per_step is the spacing"},
         "e2e": e2e_v, "gpu_launches": args.steps, "roofline": roof,
         "cpu_baseline": cpu_baseline(), "clocks": clk, "detail": detail,
     }

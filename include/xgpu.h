@@ -309,6 +309,10 @@ int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGP
  * and the fastest setting is kept. */
 int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);
 
+/* The setting in use (as xgpuTune takes it; ksplit >= 1), e.g. to keep an
+ * autotuned choice and pass it to xgpuTune in a later run. */
+int xgpuTuning(XGPUContext *context, int *ksplit, int *grid, int *pair);
+
 /* Extension for testing a caller's error handling.  While enabled, the
  * tensor-core engine of this context issues no input loads, so its bounded
  * device waits expire (about 2 s per launch) instead of completing: the next

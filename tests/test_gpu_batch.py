@@ -86,10 +86,15 @@ def test_pair_kernel_small_grid_and_autotune(xg, oracle_mod):
     exact = oracle_mod.xengine_i64(x, n, f, t)
     with xg.Correlator(n, f, t, engine="tensor") as c:
         c.tune(3, 10, 1)                  # 5 clusters walk all items
+        assert c.tuning() == {"ksplit": 3, "grid": 10, "pair": 1}
         c.set_input(x)
         c.run(xg.SYNCOP_SYNC_COMPUTE)
         assert np.array_equal(c.dump_int64(), exact)
         c.tune(0)                         # autotune over both kernels
+        got = c.tuning()
+        assert got["ksplit"] >= 1 and got["pair"] in (0, 1, 2) and got["grid"] >= 0
+        c.tune(got["ksplit"], got["grid"], got["pair"])   # a kept choice round-trips
+        assert c.tuning() == got
         c.clear()
         c.set_input(x)
         c.run(xg.SYNCOP_SYNC_COMPUTE)

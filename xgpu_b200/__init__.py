@@ -149,6 +149,8 @@ _PROTOTYPES = [
                                           ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int]),
     ("xgpuSetComputeStream", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_void_p]),
     ("xgpuComputeStream", ctypes.c_void_p, [ctypes.POINTER(XGPUContext)]),
+    ("xgpuTuning", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("xgpuEngineName", ctypes.c_char_p, [ctypes.POINTER(XGPUContext)]),
     ("xgpuCorrelateStatic", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(XGPUConfig), ctypes.c_int,
@@ -312,6 +314,13 @@ class Correlator:
         return check("xgpuSetComputeStream",
                      lib().xgpuSetComputeStream(ctypes.byref(self.ctx),
                                                 ctypes.c_void_p(stream_handle)))
+
+    def tuning(self):
+        """The tensor-engine setting in use: {"ksplit", "grid", "pair"}."""
+        k, g, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check("xgpuTuning", lib().xgpuTuning(ctypes.byref(self.ctx), ctypes.byref(k),
+                                             ctypes.byref(g), ctypes.byref(p)))
+        return {"ksplit": k.value, "grid": g.value, "pair": p.value}
 
     @property
     def stream(self):

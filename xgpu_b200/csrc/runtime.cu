@@ -723,18 +723,22 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
     t.ksplit = cand < 12 ? splits[cand % 6] : 1;
     t.wide = cand < 12 ? cand / 6 : 0;
     t.streamk = cand == 12 ? 1 : 0;
-    auto run = [&]() {
+    // Timed as calls run: on the context's own stream an accumulating launch
+    // overlaps the previous one (the first launch of a candidate does not).
+    const int chain = in->s_comp == in->s_own ? 1 : 0;
+    auto run = [&](int overlap) {
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-        if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t, 0) !=
-            cudaSuccess)
+        if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t,
+                            overlap) != cudaSuccess)
           return false;
+        overlap = chain;
       }
       return true;
     };
-    if (!run()) { rc = XGPU_CUDA_ERROR; break; }
+    if (!run(0)) { rc = XGPU_CUDA_ERROR; break; }
     cudaEventRecord(e0, in->s_comp);
-    for (int r = 0; r < 5; ++r) run();
+    for (int r = 0; r < 5; ++r) run(chain);
     cudaEventRecord(e1, in->s_comp);
     if (cudaEventSynchronize(e1) != cudaSuccess) { rc = XGPU_CUDA_ERROR; break; }
     float ms = 0.f;
@@ -750,6 +754,16 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   if (rc != XGPU_OK) return rc;
   in->tune = best_t;
   return check_device_error(in);
+}
+
+int xgpuTuning(XGPUContext *context, int *ksplit, int *grid, int *pair) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  if (!ksplit || !grid || !pair) return XGPU_INVALID_ARGUMENT;
+  *ksplit = in->tune.ksplit < 1 ? 1 : in->tune.ksplit;
+  *grid = in->tune.grid;
+  *pair = in->tune.wide ? 1 : (in->tune.streamk ? 2 : 0);
+  return XGPU_OK;
 }
 
 int xgpuInjectTimeout(XGPUContext *context, int enable) {
