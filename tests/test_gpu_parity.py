@@ -132,6 +132,30 @@ def test_exact_past_int32(xg, oracle_mod, engine):
     assert np.array_equal(out, want.astype(np.int32))
 
 
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_float_output_relative_error_vs_fp64(xg, oracle_mod, engine):
+    """Float32 output of the integer engines: the exact int64 sums are rounded
+    to float once, at dump (round to nearest), so against the FP64 host oracle
+    the relative error of every non-zero element is at most 2^-24 (6e-8, well
+    inside 1e-6), here with sums far beyond 2^24 where float accumulation
+    would drift; zero sums stay zero.  (The other orders place the same
+    rounded words: test_orders_and_output_types.)"""
+    n, f, t = 32, 2, 32768
+    x = oracle_mod.gaussian_input(n, f, t, seed=17, sigma=40.0)
+    with xg.Correlator(n, f, t, ntimepipe=128, engine=engine, output="float32") as c:
+        c.set_input(x)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)
+        c.run(xg.SYNCOP_DUMP)
+        out = c.output_view()[: c.info.matLength * 2].astype(np.float64)
+    exact = (2 * oracle_mod.xengine_i64(x, n, f, t)).astype(np.float64)   # FP64 oracle
+    assert np.abs(exact).max() > 4 * 2**24
+    nz = exact != 0
+    rel = np.abs(out[nz] - exact[nz]) / np.abs(exact[nz])
+    assert rel.max() <= 2.0**-24
+    assert rel.max() > 0            # the sums are large enough to round
+    assert not out[~nz].any()
+
+
 @pytest.mark.parametrize("engine,compute", ENGINES)
 def test_full_range_and_known_answers(xg, oracle_mod, golden, engine, compute):
     _, arr = golden

@@ -97,8 +97,11 @@ int enqueue(XGPUBatchImpl *b, const std::vector<Job> &table, int total, Job *d_j
     if (!b->jobs[q].accumulate && !table[q].store)
       BCHECK(cudaMemsetAsync(table[q].state, 0, (size_t)b->sizes[q].state_elems * 8, b->stream));
   }
+  int max_steps = 0;
+  for (const Job &j : table) max_steps = j.steps_per_split > max_steps ? j.steps_per_split : max_steps;
   if (pair)
-    BCHECK(launch_tc2_batch(d_jobs, (int)table.size(), total, b->d_queue, b->d_err, grid, b->stream));
+    BCHECK(launch_tc2_batch(d_jobs, (int)table.size(), total, b->d_queue, b->d_err, grid, b->stream,
+                            max_steps));
   else
     BCHECK(launch_tc_batch(d_jobs, (int)table.size(), total, b->d_queue, b->d_err, grid, b->stream));
   return XGPU_OK;

@@ -34,6 +34,10 @@ namespace tc2 {
 using namespace tc;
 
 constexpr int kHalf = 128;                  // G rows per CTA; B columns per CTA
+// Items of at most this many pipeline stages use the split epilogue (their
+// drains and copies outlast their MMAs); longer ones the joint one, which
+// measured 3-10% faster there.
+constexpr int kSplitEpilogueSteps = 8;
 constexpr int kStations = kHalf / 4;        // 32 stations
 constexpr int kKt = kTcSamplesPerStage;     // samples per pipeline stage
 constexpr int kStages = 4;
@@ -58,6 +62,7 @@ struct Params {
   int *err;
   int stall;           // test switch: issue no loads (the waits on them expire)
   int overlap;         // may run alongside the previous (accumulating) launch of the stream
+  int split_epi;       // epilogue schedule: 0 joint, 1 split per warp
 };
 
 // A decoded work item, 64 bytes; the leader's scheduler writes it into both
@@ -240,9 +245,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     }
     for (int q = 0; q < kSched; ++q) {
       mbar_init(sfull0 + 8 * q, 1);
-      // leader's ring slot is free once the leader's MMA issuer and epilogue and
-      // the peer's producer and epilogue have copied the entry
-      mbar_init(sempty0 + 8 * q, 4);
+      // leader's ring slot is free once the leader's MMA issuer and epilogue
+      // (each epilogue warp under the split schedule) and the peer's producer
+      // and epilogue have copied the entry
+      mbar_init(sempty0 + 8 * q, p.split_epi ? 2 + 2 * kEpiThreads / 32 : 4);
     }
     mbar_init(mma_done, 1);
     *abort_flag = 0;
@@ -378,94 +384,182 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     }
   } else {
     // ---------------------------------------------------------- epilogue --
+    // Two schedules.  Joint: the four warps drain a column block, meet at a
+    // barrier, and warp 0 hands all 32 staging rows to the bulk-copy engine.
+    // Split (launches whose items are at most 8 pipeline stages, where the
+    // drain and copies outlast the MMAs): each warp owns its 8 stations'
+    // staging rows and its lanes 0-7 issue their copies, with no barrier
+    // between warps, so one warp's copies overlap the others' drains.
     const int ew = warp - 2;
     const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31
     const int m = quarter * 32 + lane;
     const int c = m & 1;
     const int p1 = (m >> 1) & 1;
     const int il = m >> 2;
-    const bool copier = (ew == 0);
-    for (int i = 0;; ++i) {
-      const int slot = i % kSched;
-      const bool got = leader ? mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)
-                              : mbar_wait_cluster(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
-      Item t;
-      if (got) t = ring[slot];
-      if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-      if (epi_any(!got)) {
-        if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
-        break;
-      }
-      if (ew == 0 && lane == 0) {
-        if (leader) mbar_arrive(sempty0 + 8 * slot);
-        else remote_arrive(peer_addr(sempty0 + 8 * slot, 0));
-      }
-      if (t.u >= p.total) break;
-      const int acc = i & 1;
-      const bool have = mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag);
-      if (epi_any(!have)) {
-        if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
-        break;
-      }
-      __syncwarp();
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int rb = 2 * t.R + (int)rank;    // this CTA's 32-station row block
-      const long long i_glob = (long long)rb * kStations + il;
-      for (int h = 0; h < 2; ++h) {
-        const int cb = 2 * t.C + h;          // 32-station column block
-        if (cb > rb) continue;               // above the diagonal (uniform in the CTA)
-        if (h == 1) {
-          // the staging rows of column block 2C must have been read
-          if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    if (!p.split_epi) {
+      const bool copier = (ew == 0);
+      for (int i = 0;; ++i) {
+        const int slot = i % kSched;
+        const bool got = leader ? mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)
+                                : mbar_wait_cluster(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
+        Item t;
+        if (got) t = ring[slot];
+        if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        if (epi_any(!got)) {
+          if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
+          break;
+        }
+        if (ew == 0 && lane == 0) {
+          if (leader) mbar_arrive(sempty0 + 8 * slot);
+          else remote_arrive(peer_addr(sempty0 + 8 * slot, 0));
+        }
+        if (t.u >= p.total) break;
+        const int acc = i & 1;
+        const bool have = mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag);
+        if (epi_any(!have)) {
+          if (ew == 0 && lane == 0) fail(kErrTimeoutDrain);
+          break;
+        }
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int rb = 2 * t.R + (int)rank;    // this CTA's 32-station row block
+        const long long i_glob = (long long)rb * kStations + il;
+        for (int h = 0; h < 2; ++h) {
+          const int cb = 2 * t.C + h;          // 32-station column block
+          if (cb > rb) continue;               // above the diagonal (uniform in the CTA)
+          if (h == 1) {
+            // the staging rows of column block 2C must have been read
+            if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            epi_barrier();
+          }
+          uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+          int jmax = t.n - cb * kStations;
+          if (jmax > kStations) jmax = kStations;
+          if (cb == rb && il + 1 < jmax) jmax = il + 1;
+          if (i_glob >= t.n) jmax = 0;
+          uint32_t v[kHalf / 32][32];
+          tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccCols + h * kHalf),
+                     v);
+#pragma unroll
+          for (int q = 0; q < kHalf / 32; ++q) {
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+              const int v0 = (int)v[q][4 * jj], v1 = (int)v[q][4 * jj + 1];
+              const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
+              const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
+              const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
+              const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
+              const long long im = c ? (long long)v2 - rb2 : (long long)ra - v1;
+              const int jl = q * 8 + jj;
+              if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
+            }
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           epi_barrier();
-        }
-        uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
-        int jmax = t.n - cb * kStations;
-        if (jmax > kStations) jmax = kStations;
-        if (cb == rb && il + 1 < jmax) jmax = il + 1;
-        if (i_glob >= t.n) jmax = 0;
-        uint32_t v[kHalf / 32][32];
-        tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccCols + h * kHalf),
-                   v);
-#pragma unroll
-        for (int q = 0; q < kHalf / 32; ++q) {
-#pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
-            const int v0 = (int)v[q][4 * jj], v1 = (int)v[q][4 * jj + 1];
-            const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
-            const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
-            const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
-            const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
-            const long long im = c ? (long long)v2 - rb2 : (long long)ra - v1;
-            const int jl = q * 8 + jj;
-            if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
+          if (copier) {
+            // row `lane` of the staging block -> baselines (32 rb + lane, 32 cb .. )
+            const long long ig = (long long)rb * kStations + lane;
+            int cnt = t.n - cb * kStations;
+            if (cnt > kStations) cnt = kStations;
+            if (cb == rb && lane + 1 < cnt) cnt = lane + 1;
+            if (ig >= t.n) cnt = 0;
+            if (cnt > 0) {
+              int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
+                                        (long long)cb * kStations) * 8;
+              const uint32_t src = smem_u32(sstate + lane * kRowPitch);
+              if (t.store) bulk_store(dst, src, cnt * 64);
+              else bulk_reduce_add(dst, src, cnt * 64);
+            }
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        epi_barrier();
-        if (copier) {
-          // row `lane` of the staging block -> baselines (32 rb + lane, 32 cb .. )
-          const long long ig = (long long)rb * kStations + lane;
-          int cnt = t.n - cb * kStations;
-          if (cnt > kStations) cnt = kStations;
-          if (cb == rb && lane + 1 < cnt) cnt = lane + 1;
-          if (ig >= t.n) cnt = 0;
-          if (cnt > 0) {
-            int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
-                                      (long long)cb * kStations) * 8;
-            const uint32_t src = smem_u32(sstate + lane * kRowPitch);
-            if (t.store) bulk_store(dst, src, cnt * 64);
-            else bulk_reduce_add(dst, src, cnt * 64);
+        // The accumulator has been read (or was not needed): release it.
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) remote_arrive(peer_addr(tempty0 + 8 * acc, 0));
+      }
+      if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    } else {
+      const bool copier = lane < 8;          // copies staging row crow
+      const int crow = quarter * 8 + lane;
+      for (int i = 0;; ++i) {
+        const int slot = i % kSched;
+        const bool got = leader ? mbar_wait(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag)
+                                : mbar_wait_cluster(sfull0 + 8 * slot, (i / kSched) & 1, abort_flag);
+        if (!__all_sync(0xffffffffu, got)) {
+          if (lane == 0) fail(kErrTimeoutDrain);
+          break;
+        }
+        const Item t = ring[slot];
+        __syncwarp();
+        if (lane == 0) {                     // this warp has copied the entry
+          if (leader) mbar_arrive(sempty0 + 8 * slot);
+          else remote_arrive(peer_addr(sempty0 + 8 * slot, 0));
+        }
+        if (t.u >= p.total) break;
+        const int acc = i & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(tfull0 + 8 * acc, (i >> 1) & 1, abort_flag))) {
+          if (lane == 0) fail(kErrTimeoutDrain);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int rb = 2 * t.R + (int)rank;
+        const long long i_glob = (long long)rb * kStations + il;
+        const int hlast = (2 * t.C + 1 > rb) ? 0 : 1;   // last column block at or below the diagonal
+        for (int h = 0; h <= hlast; ++h) {
+          const int cb = 2 * t.C + h;
+          uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+          int jmax = t.n - cb * kStations;
+          if (jmax > kStations) jmax = kStations;
+          if (cb == rb && il + 1 < jmax) jmax = il + 1;
+          if (i_glob >= t.n) jmax = 0;
+          uint32_t v[kHalf / 32][32];
+          tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccCols + h * kHalf),
+                     v);
+          if (h == hlast) {
+            // The accumulator has been read: release it to the leader's MMA issuer.
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) remote_arrive(peer_addr(tempty0 + 8 * acc, 0));
           }
-          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          // This warp's staging rows are free once its previous copies have read them.
+          if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          __syncwarp();
+#pragma unroll
+          for (int q = 0; q < kHalf / 32; ++q) {
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+              const int v0 = (int)v[q][4 * jj], v1 = (int)v[q][4 * jj + 1];
+              const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
+              const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
+              const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
+              const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
+              const long long im = c ? (long long)v2 - rb2 : (long long)ra - v1;
+              const int jl = q * 8 + jj;
+              if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
+            }
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (copier) {
+            const long long ig = (long long)rb * kStations + crow;
+            int cnt = t.n - cb * kStations;
+            if (cnt > kStations) cnt = kStations;
+            if (cb == rb && crow + 1 < cnt) cnt = crow + 1;
+            if (ig >= t.n) cnt = 0;
+            if (cnt > 0) {
+              int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
+                                        (long long)cb * kStations) * 8;
+              const uint32_t src = smem_u32(sstate + crow * kRowPitch);
+              if (t.store) bulk_store(dst, src, cnt * 64);
+              else bulk_reduce_add(dst, src, cnt * 64);
+            }
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
         }
       }
-      // The accumulator has been read (or was not needed): release it.
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) remote_arrive(peer_addr(tempty0 + 8 * acc, 0));
+      if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
-    if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 
   __syncwarp();   // lanes 1-31 of the producer and MMA warps wait for lane 0
@@ -530,6 +624,7 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   p.err = err;
   p.stall = tune.stall;
   p.overlap = (overlap && !overwrite) ? 1 : 0;
+  p.split_epi = per <= tc2::kSplitEpilogueSteps ? 1 : 0;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
   if (clusters > p.total) clusters = p.total;
   if (clusters < 1) clusters = 1;
@@ -549,7 +644,7 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
 }
 
 cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
-                             int grid, cudaStream_t st) {
+                             int grid, cudaStream_t st, int max_item_steps) {
   int dev = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -570,6 +665,7 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
   p.err = err;
   p.stall = 0;
   p.overlap = 0;
+  p.split_epi = max_item_steps <= tc2::kSplitEpilogueSteps ? 1 : 0;
   int clusters = (grid > 0 ? grid : sms) / 2;
   if (clusters > total_items) clusters = total_items;
   if (clusters < 1) return cudaSuccess;

@@ -78,9 +78,11 @@ cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int
 // 256x256 tiles of the CTA-pair kernel.  Returns 0 on success.
 int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount, int64_t *state,
                 int store, int ksplit, int item_begin, int pair);
-// The CTA-pair kernel over a device job table filled with pair = 1.
+// The CTA-pair kernel over a device job table filled with pair = 1;
+// max_item_steps is the largest steps_per_split in the table (it selects the
+// epilogue schedule).
 cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
-                             int grid, cudaStream_t st);
+                             int grid, cudaStream_t st, int max_item_steps);
 // Encodes the 3-D tensor map {x: 4n bytes, y: f, z: t} over a device input
 // buffer.  Returns 0 on success.
 int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);

@@ -716,13 +716,33 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   TcTuning best_t = in->tune;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, in->device);
+  // Candidates: single CTAs and CTA pairs with 1-8 time splits on every SM,
+  // stream-K, and smaller grids, which pay off when consecutive calls overlap
+  // (each call then runs on part of the GPU with more tiles per CTA, so the
+  // per-CTA prologue and last drain are spread thinner).
+  struct Cand {
+    int ksplit, grid, wide, streamk;
+  };
+  Cand cands[24];
+  int ncand = 0;
   const int splits[] = {1, 2, 3, 4, 6, 8};
+  for (int wide = 0; wide < 2; ++wide)
+    for (int q = 0; q < 6; ++q) cands[ncand++] = {splits[q], 0, wide, 0};
+  cands[ncand++] = {1, 0, 0, 1};
+  if (sms >= 16) {
+    for (int d : {2, 4, 6, 8}) cands[ncand++] = {1, sms / d, 0, 0};
+    cands[ncand++] = {2, sms / 2, 0, 0};
+    cands[ncand++] = {2, sms / 4, 0, 0};
+    cands[ncand++] = {1, sms / 2, 1, 0};
+    cands[ncand++] = {1, sms / 4, 1, 0};
+  }
   int rc = XGPU_OK;
-  for (int cand = 0; cand < 13; ++cand) {
+  for (int ci = 0; ci < ncand; ++ci) {
     TcTuning t;
-    t.ksplit = cand < 12 ? splits[cand % 6] : 1;
-    t.wide = cand < 12 ? cand / 6 : 0;
-    t.streamk = cand == 12 ? 1 : 0;
+    t.ksplit = cands[ci].ksplit;
+    t.grid = cands[ci].grid;
+    t.wide = cands[ci].wide;
+    t.streamk = cands[ci].streamk;
     // Timed as calls run: on the context's own stream an accumulating launch
     // overlaps the previous one (the first launch of a candidate does not).
     const int chain = in->s_comp == in->s_own ? 1 : 0;
@@ -736,13 +756,23 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
       }
       return true;
     };
-    if (!run(0)) { rc = XGPU_CUDA_ERROR; break; }
+    // One warm run sizes the repetitions: enough for the overlap to settle
+    // (up to 16), about 2 ms of work per candidate, at least 3.
     cudaEventRecord(e0, in->s_comp);
-    for (int r = 0; r < 5; ++r) run(chain);
+    if (!run(0)) { rc = XGPU_CUDA_ERROR; break; }
+    cudaEventRecord(e1, in->s_comp);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = XGPU_CUDA_ERROR; break; }
+    float one = 0.f;
+    cudaEventElapsedTime(&one, e0, e1);
+    int reps = one > 0.f ? (int)(2.0f / one) : 16;
+    reps = reps < 3 ? 3 : (reps > 16 ? 16 : reps);
+    cudaEventRecord(e0, in->s_comp);
+    for (int r = 0; r < reps; ++r) run(chain);
     cudaEventRecord(e1, in->s_comp);
     if (cudaEventSynchronize(e1) != cudaSuccess) { rc = XGPU_CUDA_ERROR; break; }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
+    ms /= (float)reps;
     if (ms < best) {
       best = ms;
       best_t = t;

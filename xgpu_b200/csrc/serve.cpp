@@ -418,7 +418,11 @@ extern "C" int xgpuServeRun(const XGPUServeJob *jobs, int njobs, const XGPUServe
         if (!plain) {
           Job *dtab = d_tables + (size_t)table_slot * max_table;
           SCHECK(cudaMemcpyAsync(dtab, tab, sizeof(Job) * nent, cudaMemcpyHostToDevice, s_step));
-          SCHECK(launch_tc2_batch(dtab, nent, items, d_queue + table_slot, d_err, sms, s_step));
+          int max_steps = 0;
+          for (int q = 0; q < nent; ++q)
+            max_steps = tab[q].steps_per_split > max_steps ? tab[q].steps_per_split : max_steps;
+          SCHECK(launch_tc2_batch(dtab, nent, items, d_queue + table_slot, d_err, sms, s_step,
+                                  max_steps));
         }
         table_slot = (table_slot + 1) % kTables;
         for (const auto &rq : ready) {

@@ -1,8 +1,8 @@
 """Time one engine on one shape with the input resident in device memory.
 
     python -m xgpu_b200.profile_case --n 512 --f 32 --t 8192 [--engine tensor|plain|fp32]
-                                     [--reps 5] [--warmup 3] [--ksplit K] [--accumulate]
-                                     [--caller-stream]
+                                     [--reps 5] [--warmup 3] [--ksplit K] [--pair P]
+                                     [--grid G] [--accumulate] [--caller-stream]
 
 Prints one JSON line: milliseconds per xgpuCudaXengineDevice call (CUDA
 events on the engine's stream), X-engine TOPS (16*F*T*N(N+1) ops per call)
@@ -26,7 +26,9 @@ def main():
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--ksplit", type=int, default=-1, help="-1: engine default, 0: autotune")
-    ap.add_argument("--pair", type=int, default=0, help="1: CTA-pair kernel (256x256 tiles)")
+    ap.add_argument("--pair", type=int, default=0,
+                    help="1: CTA-pair kernel (256x256 tiles), 2: stream-K")
+    ap.add_argument("--grid", type=int, default=0, help="CTAs per launch (0: one per SM)")
     ap.add_argument("--accumulate", action="store_true",
                     help="add into the integration (default: every call starts a new one)")
     ap.add_argument("--sigma", type=float, default=16.0)
@@ -39,8 +41,8 @@ def main():
     engine = "plain" if args.engine in ("plain", "fp32") else "tensor"
     c = xg.Correlator(args.n, args.f, args.t, ntimepipe=16, engine=engine, compute=compute,
                       output="int32" if compute == "int8" else "float32", order="tri")
-    if args.ksplit >= 0 or args.pair:
-        c.tune(max(args.ksplit, 0) if args.ksplit != -1 else 1, 0, args.pair)
+    if args.ksplit >= 0 or args.pair or args.grid:
+        c.tune(max(args.ksplit, 0) if args.ksplit != -1 else 1, args.grid, args.pair)
     if args.caller_stream:
         stream = torch.cuda.Stream()
         c.set_stream(stream.cuda_stream)
@@ -66,9 +68,10 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.reps
     ops = xg.ops_per_integration(args.n, args.f, args.t)
+    tuning = c.tuning() if engine == "tensor" else None
     print(json.dumps({"engine": c.engine_name, "n": args.n, "f": args.f, "t": args.t,
                       "ms": ms, "tops": ops / (ms * 1e-3) / 1e12, "host_enqueue_ms": host_ms,
-                      "accumulate": args.accumulate}))
+                      "accumulate": args.accumulate, "tuning": tuning}))
     c.close()
 
 
