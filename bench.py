@@ -56,9 +56,10 @@ def load_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback (no MEASURED_PEAKS.json)"
 
 
-def read_profile_traffic():
-    """Per-launch DRAM bytes of the tensor kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "xengine_tc_kernel_n256.md")
+def read_profile_traffic(pair):
+    """Per-launch DRAM bytes of the headline kernel from its committed ncu summary."""
+    name = "xengine_tc2_kernel_n256.md" if pair == 1 else "xengine_tc_kernel_n256.md"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -554,9 +555,11 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     t_hbm = alg_bytes / (hbm_peak * 1e9)
     t_tc = ops(N, F, T) / ((peak8 or 2 * float(peaks.get("bf16_tflops", 1590.0))) * 1e12)
-    traffic = read_profile_traffic()
+    tuning = TUNING.get(("tensor", N, F, T)) or {}
+    traffic = read_profile_traffic(tuning.get("pair", 0))
+    kernel = "xengine_tc2_kernel" if tuning.get("pair", 0) == 1 else "xengine_tc_kernel"
     if t_hbm >= t_tc:
-        roof = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
+        roof = {"bound": "hbm", "kernel": kernel, "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
                 "frac": hbm_ach / hbm_peak, "traffic": traffic,
                 "peak_source": f"hbm_gbs of {peak_src} (of measured)",
                 "algorithmic_bytes_per_launch": alg_bytes,
@@ -564,7 +567,7 @@ def main():
                         "stays in L2 between calls, so DRAM sees less (traffic: ncu, cold "
                         "stand-alone launch)"}
     else:
-        roof = {"bound": "tensor", "achieved": tops_ach, "peak": peak8, "unit": "TOPS",
+        roof = {"bound": "tensor", "kernel": kernel, "achieved": tops_ach, "peak": peak8, "unit": "TOPS",
                 "frac": tops_ach / peak8, "traffic": traffic,
                 "peak_source": "dense int8 cuBLASLt GEMM 8192^3 measured in this run (of measured)"}
     detail["int8_tensor_peak_tops_measured"] = peak8
