@@ -28,7 +28,7 @@ def test_reference_driver_self_check(args):
 
 def test_reference_driver_streaming_calls():
     """Several calls per integration with SYNCOP_NONE / SYNCOP_SYNC_TRANSFER
-    (the driver checks only single-call integrations, so this checks that the
+    (xGPU's test program checks only single-call integrations, so this checks that the
     pipelined calling pattern runs cleanly)."""
     if not os.path.exists(EXE):
         pytest.skip("reference driver not built")

@@ -390,3 +390,29 @@ def test_overlapping_calls_of_several_segments(xg, oracle_mod):
         got = c.dump_int64()
     want = 2 * sum(oracle_mod.xengine_i64(x, n, f, t) for x in xs)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("pair", [0, 1])
+def test_long_overlapping_integration_past_int32(xg, oracle_mod, pair):
+    """70 full-scale calls of 1024 samples overlapping on the device (sums past
+    2^31) stay exact in int64, and three more after a dump too; the int32 dump
+    wraps like xGPU's int32 buffer."""
+    import torch
+    n, f, t = 32, 2, 1024
+    x = np.empty(t * f * n * 4, dtype=np.int8)
+    x[0::2] = -128
+    x[1::2] = 127
+    x[5::16] = 3
+    d = torch.from_numpy(x).cuda()
+    torch.cuda.synchronize()
+    one = oracle_mod.xengine_i64(x, n, f, t)
+    with xg.Correlator(n, f, t, engine="tensor", output="int32") as c:
+        c.tune(1, 0, pair)
+        for _ in range(70):
+            c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        got = c.dump_int64()
+        assert np.abs(got).max() > 2**31
+        assert np.array_equal(got, 70 * one)
+        for _ in range(3):
+            c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        assert np.array_equal(c.dump(), (73 * one).astype(np.int32))
