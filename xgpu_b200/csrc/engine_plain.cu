@@ -59,6 +59,7 @@ struct Params {
   long long nbaseline;
   void *state;
   int overwrite;
+  int per;        // samples per time split (blockIdx.z); == tcount without splits
 };
 
 // Issue the cp.async loads of samples [tb, tb+nt) of one panel (32 stations
@@ -119,8 +120,10 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const Params 
   decode_block(blockIdx.x, rb, cb);
   const bool diag = (rb == cb);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int tend = p.t0 + p.tcount;
-  const int nchunks = (p.tcount + kTcD - 1) / kTcD;
+  // Time split blockIdx.z covers samples [tbeg, tend) of the call's range.
+  const int tbeg = p.t0 + (int)blockIdx.z * p.per;
+  const int tend = min(p.t0 + p.tcount, tbeg + p.per);
+  const int nchunks = (tend - tbeg + kTcD - 1) / kTcD;
 
   int re[2][2][2][2], i1[2][2][2][2], i2[2][2][2][2];   // [rs][cs][p1][p2]
 #pragma unroll
@@ -130,14 +133,14 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const Params 
     (&i2[0][0][0][0])[a] = 0;
   }
 
-  load_panel<kTcD>(raw[0][0], p, f, rb * kBlk, p.t0, tend);
-  if (!diag) load_panel<kTcD>(raw[0][1], p, f, cb * kBlk, p.t0, tend);
+  load_panel<kTcD>(raw[0][0], p, f, rb * kBlk, tbeg, tend);
+  if (!diag) load_panel<kTcD>(raw[0][1], p, f, cb * kBlk, tbeg, tend);
   cp_async_commit();
 
   for (int ch = 0; ch < nchunks; ++ch) {
     const int buf = ch & 1;
     if (ch + 1 < nchunks) {
-      const int tb = p.t0 + (ch + 1) * kTcD;
+      const int tb = tbeg + (ch + 1) * kTcD;
       load_panel<kTcD>(raw[buf ^ 1][0], p, f, rb * kBlk, tb, tend);
       if (!diag) load_panel<kTcD>(raw[buf ^ 1][1], p, f, cb * kBlk, tb, tend);
       cp_async_commit();
@@ -194,7 +197,11 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const Params 
           const long long vr = re[rs][cs][p1][p2];
           const long long vi = (long long)i1[rs][cs][p1][p2] - (long long)i2[rs][cs][p1][p2];
           longlong2 *d = dst + p1 * 2 + p2;
-          if (p.overwrite) {
+          if (gridDim.z > 1) {
+            // Time splits of one block add exactly, in any order.
+            atomicAdd((unsigned long long *)&d->x, (unsigned long long)vr);
+            atomicAdd((unsigned long long *)&d->y, (unsigned long long)vi);
+          } else if (p.overwrite) {
             *d = make_longlong2(vr, vi);
           } else {
             longlong2 o = *d;
@@ -315,21 +322,65 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const Params p) 
 
 }  // namespace plain
 
-static dim3 plain_grid(const Sizes &s) {
+static dim3 plain_grid(const Sizes &s, int ksplit = 1) {
   const int nb = (s.n + plain::kBlk - 1) / plain::kBlk;
-  return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)s.f);
+  return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)s.f, (unsigned)ksplit);
+}
+
+// Time splits for the dp4a kernel: with fewer 32x32-station blocks than a few
+// waves of resident CTAs (two per SM), the last wave runs half empty (at N=256,
+// F=10: 360 blocks on 296 slots is 61% busy).  Pick the split count, from 1
+// to 16, whose whole number of waves is fullest, keeping at least 512 samples
+// per split: each split adds its 8192 sums per block with int64 atomics, and
+// shorter splits lost more to those than they gained (N=256, F=10, T=1024:
+// 155 us unsplit, 137 us with 2 splits, 153 us with 4).  Launches of fewer
+// than 64 blocks are latency-bound and are not split (N=64, F=10, T=1024:
+// 27 us unsplit, 35 us with 2 splits).
+static int plain_splits(const Sizes &s, int tcount) {
+  static int slots = 0;
+  if (!slots) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return 1;
+    slots = 2 * sms;
+  }
+  const dim3 g = plain_grid(s);
+  const long long blocks = (long long)g.x * g.y;
+  if (blocks >= 4LL * slots || blocks < 64) return 1;
+  int best = 1;
+  double best_fill = 0.0;
+  for (int k = 1; k <= 16 && (k == 1 || tcount / k >= 512); ++k) {
+    const long long ctas = blocks * k;
+    const long long waves = (ctas + slots - 1) / slots;
+    const double fill = (double)ctas / (double)(waves * slots);
+    if (fill > best_fill + 0.02) {
+      best_fill = fill;
+      best = k;
+    }
+  }
+  return best;
 }
 
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
                               int64_t *state, int overwrite, cudaStream_t st) {
-  plain::Params p{in, s.n, s.f, t0, tcount, s.nbaseline, state, overwrite};
-  plain::xengine_dp4a_kernel<<<plain_grid(s), plain::kThreads, 0, st>>>(p);
+  const int ks = plain_splits(s, tcount);
+  // samples per split: a whole number of 64-sample chunks
+  int per = (tcount + ks - 1) / ks;
+  per = (per + plain::kTcD - 1) / plain::kTcD * plain::kTcD;
+  const int used = (tcount + per - 1) / per;
+  if (used > 1 && overwrite) {
+    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
+    if (e != cudaSuccess) return e;
+  }
+  plain::Params p{in, s.n, s.f, t0, tcount, s.nbaseline, state, overwrite, per};
+  plain::xengine_dp4a_kernel<<<plain_grid(s, used), plain::kThreads, 0, st>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount, float *state,
                               int overwrite, cudaStream_t st) {
-  plain::Params p{in, s.n, s.f, t0, tcount, s.nbaseline, state, overwrite};
+  plain::Params p{in, s.n, s.f, t0, tcount, s.nbaseline, state, overwrite, tcount};
   plain::xengine_fp32_kernel<<<plain_grid(s), plain::kThreads, 0, st>>>(p);
   return cudaGetLastError();
 }
