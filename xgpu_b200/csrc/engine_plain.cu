@@ -327,15 +327,13 @@ static dim3 plain_grid(const Sizes &s, int ksplit = 1) {
   return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)s.f, (unsigned)ksplit);
 }
 
-// Time splits for the dp4a kernel: with fewer 32x32-station blocks than a few
-// waves of resident CTAs (two per SM), the last wave runs half empty (at N=256,
-// F=10: 360 blocks on 296 slots is 61% busy).  Pick the split count, from 1
-// to 16, whose whole number of waves is fullest, keeping at least 512 samples
-// per split: each split adds its 8192 sums per block with int64 atomics, and
-// shorter splits lost more to those than they gained (N=256, F=10, T=1024:
-// 155 us unsplit, 137 us with 2 splits, 153 us with 4).  Launches of fewer
-// than 64 blocks are latency-bound and are not split (N=64, F=10, T=1024:
-// 27 us unsplit, 35 us with 2 splits).
+// Time splits for the dp4a kernel.  With fewer 32x32-station blocks than two
+// waves of resident CTAs (two per SM), SMs idle: at N=256, F=10 the 360 blocks
+// leave the second wave mostly empty, and at N=64 the 30 blocks occupy a fifth
+// of the GPU.  Split each block's samples until there are about two waves,
+// keeping at least 256 samples per split and at most 8 splits (each split adds
+// its 8192 sums per block with int64 atomics).  Measured at F=10, T=1024:
+// N=256 155 -> 137 us (2 splits), N=64 60 -> 27 us (4 splits).
 static int plain_splits(const Sizes &s, int tcount) {
   static int slots = 0;
   if (!slots) {
@@ -347,19 +345,10 @@ static int plain_splits(const Sizes &s, int tcount) {
   }
   const dim3 g = plain_grid(s);
   const long long blocks = (long long)g.x * g.y;
-  if (blocks >= 4LL * slots || blocks < 64) return 1;
-  int best = 1;
-  double best_fill = 0.0;
-  for (int k = 1; k <= 16 && (k == 1 || tcount / k >= 512); ++k) {
-    const long long ctas = blocks * k;
-    const long long waves = (ctas + slots - 1) / slots;
-    const double fill = (double)ctas / (double)(waves * slots);
-    if (fill > best_fill + 0.02) {
-      best_fill = fill;
-      best = k;
-    }
-  }
-  return best;
+  long long k = (2LL * slots + blocks - 1) / blocks;
+  if (k > tcount / 256) k = tcount / 256;
+  if (k > 8) k = 8;
+  return k < 1 ? 1 : (int)k;
 }
 
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,

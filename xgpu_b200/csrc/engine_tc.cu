@@ -21,7 +21,7 @@
 // global atomic work queue (uneven batches); the producer publishes each item
 // to the other roles through a small shared-memory ring.  Six warps:
 //   warp 0    scheduler + TMA producer: 3-D tiled loads (128 bytes x 128
-//             samples, 128-byte swizzle) of row and column panels, 4 stages
+//             samples, 128-byte swizzle) of row and column panels, 5 stages
 //   warp 1    TMEM owner and MMA issuer: tcgen05.mma.cta_group::1.kind::i8,
 //             M=N=128, K=32, into one of two TMEM accumulators (2 x 128
 //             columns), so a tile's drain overlaps the next tile's MMAs
@@ -48,14 +48,18 @@ namespace tc {
 constexpr int kTile = 128;                 // G rows (and columns) per tile
 constexpr int kStations = kTile / 4;       // 32 stations per tile side
 constexpr int kKt = kTcSamplesPerStage;    // samples per pipeline stage
-constexpr int kStages = 4;
+constexpr int kStages = 5;
 constexpr int kSched = 4;                  // work-item ring between the roles
 constexpr int kBoxBytes = kTile * kKt;     // one operand of one stage: 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;
-constexpr int kRowPitch = kStations * 64 + 64;   // one station row of the staging tile, padded
+// One station row of the staging tile; 16 bytes of padding put the 8 rows a
+// warp writes on distinct 16-byte bank groups, and five 32 KB stages still
+// fit in 227 KB.
+constexpr int kRowPitch = kStations * 64 + 16;
 constexpr int kStateBytes = kStations * kRowPitch;
-constexpr int kBarrierBytes = 1024;
+constexpr int kBarrierBytes = 512;    // barriers, work-item ring, TMEM slot
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
+static_assert(kSmemBytes <= 227 * 1024, "dynamic shared memory of one CTA");
 constexpr uint32_t kTmemCols = 2 * kTile;  // two accumulators
 constexpr int kThreads = 192;
 

@@ -40,14 +40,17 @@ constexpr int kHalf = 128;                  // G rows per CTA; B columns per CTA
 constexpr int kSplitEpilogueSteps = 8;
 constexpr int kStations = kHalf / 4;        // 32 stations
 constexpr int kKt = kTcSamplesPerStage;     // samples per pipeline stage
-constexpr int kStages = 4;
+constexpr int kStages = 5;
 constexpr int kSched = 4;
 constexpr int kBoxBytes = kHalf * kKt;      // 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;  // A rows + B half
-constexpr int kRowPitch = kStations * 64 + 64;
+// 16 bytes of padding per 2 KB row: the 8 rows a warp writes fall on distinct
+// 16-byte bank groups, and five 32 KB stages still fit in 227 KB.
+constexpr int kRowPitch = kStations * 64 + 16;
 constexpr int kStateBytes = kStations * kRowPitch;   // one 32x32-station block
-constexpr int kBarrierBytes = 1024;
+constexpr int kBarrierBytes = 512;    // barriers, work-item ring, TMEM slot
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
+static_assert(kSmemBytes <= 227 * 1024, "dynamic shared memory of one CTA");
 constexpr uint32_t kAccCols = 2 * kHalf;    // 256 columns per accumulator
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kThreads = 192;
