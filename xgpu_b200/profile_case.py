@@ -3,6 +3,7 @@
     python -m xgpu_b200.profile_case --n 512 --f 32 --t 8192 [--engine tensor|plain|fp32]
                                      [--reps 5] [--warmup 3] [--ksplit K] [--pair P]
                                      [--grid G] [--accumulate] [--caller-stream]
+                                     [--format int8|packed4|dp4a_swizzled|block32] [--dump]
 
 Prints one JSON line: milliseconds per xgpuCudaXengineDevice call (CUDA
 events on the engine's stream), X-engine TOPS (16*F*T*N(N+1) ops per call)
@@ -34,13 +35,18 @@ def main():
     ap.add_argument("--sigma", type=float, default=16.0)
     ap.add_argument("--caller-stream", action="store_true",
                     help="run on a caller stream (xgpuSetComputeStream) instead of the context's")
+    ap.add_argument("--format", default="int8", choices=sorted(xg.FORMATS),
+                    help="input format (converted on the device before the engine)")
+    ap.add_argument("--dump", action="store_true",
+                    help="dump (device formatting + copy to the host) after every call")
     args = ap.parse_args()
 
     import torch
     compute = "fp32" if args.engine == "fp32" else "int8"
     engine = "plain" if args.engine in ("plain", "fp32") else "tensor"
     c = xg.Correlator(args.n, args.f, args.t, ntimepipe=16, engine=engine, compute=compute,
-                      output="int32" if compute == "int8" else "float32", order="tri")
+                      output="int32" if compute == "int8" else "float32", order="tri",
+                      input_format=args.format)
     if args.ksplit >= 0 or args.pair or args.grid:
         c.tune(max(args.ksplit, 0) if args.ksplit != -1 else 1, args.grid, args.pair)
     if args.caller_stream:
@@ -48,13 +54,16 @@ def main():
         c.set_stream(stream.cuda_stream)
     else:
         stream = torch.cuda.ExternalStream(c.stream)
-    nbytes = int(c.info.vecLength) * 2
+    packed = args.format == "packed4"
+    nbytes = int(c.info.vecLength) * (1 if packed else 2)
     x = torch.empty(nbytes, dtype=torch.int8, device="cuda")
-    xg.generate_device(x.data_ptr(), nbytes, 0, 7, args.sigma, torch.cuda.current_device())
+    xg.generate_device(x.data_ptr(), nbytes, 1 if packed else 0, 7, args.sigma,
+                       torch.cuda.current_device())
+    sync = xg.SYNCOP_DUMP if args.dump else xg.SYNCOP_NONE
     for _ in range(args.warmup):
         if not args.accumulate:
             c.clear()
-        c.run_device(x.data_ptr(), xg.SYNCOP_NONE)
+        c.run_device(x.data_ptr(), sync)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -62,7 +71,7 @@ def main():
     for _ in range(args.reps):
         if not args.accumulate:
             c.clear()
-        c.run_device(x.data_ptr(), xg.SYNCOP_NONE)
+        c.run_device(x.data_ptr(), sync)
     host_ms = (time.perf_counter() - h0) * 1e3 / args.reps
     e1.record(stream)
     torch.cuda.synchronize()
