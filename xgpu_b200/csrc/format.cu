@@ -68,38 +68,45 @@ __global__ void format_kernel(const Params p) {
   }
 }
 
-// Packed 4+4-bit -> int8 pairs: 4 samples (one 32-bit word) per iteration.
-__global__ void unpack4_kernel(const uint32_t *in, uint2 *out, long long nwords) {
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nwords;
+// Four packed 4+4-bit samples (re high nibble, im low nibble, two's
+// complement) -> eight int8 bytes {re, im} in the same order.  Byte-wise:
+// a nibble v in 0..15 is the signed value (v ^ 8) - 8.
+__device__ __forceinline__ uint2 expand4(uint32_t w) {
+  const uint32_t re = __vsub4(((w >> 4) & 0x0F0F0F0Fu) ^ 0x08080808u, 0x08080808u);
+  const uint32_t im = __vsub4((w & 0x0F0F0F0Fu) ^ 0x08080808u, 0x08080808u);
+  return make_uint2(__byte_perm(re, im, 0x5140), __byte_perm(re, im, 0x7362));
+}
+
+// 16 packed samples per thread: one 16-byte load, two 16-byte stores.
+__global__ void unpack4_kernel(const uint4 *in, uint4 *out, long long nquads) {
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nquads;
        u += (long long)gridDim.x * blockDim.x) {
-    const uint32_t w = in[u];
-    uint32_t o[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      uint32_t acc = 0;
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const int byte = (int)((w >> (8 * (2 * h + b))) & 0xFF);
-        const int re = ((int)(int8_t)byte) >> 4;
-        const int im = ((int)(int8_t)(byte << 4)) >> 4;
-        acc |= ((uint32_t)(re & 0xFF) | ((uint32_t)(im & 0xFF) << 8)) << (16 * b);
-      }
-      o[h] = acc;
-    }
-    out[u] = make_uint2(o[0], o[1]);
+    const uint4 w = in[u];
+    const uint2 a = expand4(w.x), b = expand4(w.y), c = expand4(w.z), d = expand4(w.w);
+    out[2 * u] = make_uint4(a.x, a.y, b.x, b.y);
+    out[2 * u + 1] = make_uint4(c.x, c.y, d.x, d.y);
   }
 }
 
-// [t/4][f][s][p][c][t%4] -> [t][f][s][p][c] (inverse of cpu_util.c:235-255).
-__global__ void unswizzle_kernel(const uint32_t *in, int8_t *out, long long groups,
-                                 long long row_bytes) {
-  // groups = (t/4) * f * n * 4 entries of 4 bytes; row_bytes = f*n*4
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < groups;
+// xgpuSwizzleInput's layout (cpu_util.c:235-255) back to [t][f][s][p][c]:
+// byte e of row-group tq holds samples 4tq..4tq+3 of input byte e.  One thread
+// takes 16 bytes (input bytes 4e4..4e4+3, four samples each), transposes them
+// 4x4 with byte permutes, and writes one 4-byte word to each of the four
+// sample rows (consecutive threads write consecutive words of a row).
+__global__ void unswizzle_kernel(const uint4 *in, uint32_t *out, long long quads,
+                                 long long row_words) {
+  // quads = (t/4) * row_words; row_words = f*n (4 bytes per station)
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < quads;
        u += (long long)gridDim.x * blockDim.x) {
-    const long long tq = u / row_bytes, e = u - tq * row_bytes;
-    const uint32_t w = in[u];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) out[(4 * tq + r) * row_bytes + e] = (int8_t)((w >> (8 * r)) & 0xFF);
+    const long long tq = u / row_words, e4 = u - tq * row_words;
+    const uint4 w = in[u];
+    const uint32_t lo01 = __byte_perm(w.x, w.y, 0x5140), hi01 = __byte_perm(w.x, w.y, 0x7362);
+    const uint32_t lo23 = __byte_perm(w.z, w.w, 0x5140), hi23 = __byte_perm(w.z, w.w, 0x7362);
+    uint32_t *o = out + 4 * tq * row_words + e4;
+    o[0] = __byte_perm(lo01, lo23, 0x5410);
+    o[row_words] = __byte_perm(lo01, lo23, 0x7632);
+    o[2 * row_words] = __byte_perm(hi01, hi23, 0x5410);
+    o[3 * row_words] = __byte_perm(hi01, hi23, 0x7632);
   }
 }
 
@@ -198,18 +205,18 @@ cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s,
 }
 
 cudaError_t launch_unpack4(const uint8_t *in, int8_t *out, long long nsamples, cudaStream_t st) {
-  const long long nwords = nsamples / 4;  // nsamples is a multiple of 8 (n % 16 == 0)
-  fmt::unpack4_kernel<<<fmt::grid_for(nwords, 256), 256, 0, st>>>((const uint32_t *)in,
-                                                                  (uint2 *)out, nwords);
+  const long long nquads = nsamples / 16;  // nsamples = 2*n*f*t, a multiple of 32 (n % 16 == 0)
+  fmt::unpack4_kernel<<<fmt::grid_for(nquads, 256), 256, 0, st>>>((const uint4 *)in,
+                                                                  (uint4 *)out, nquads);
   return cudaGetLastError();
 }
 
 cudaError_t launch_unswizzle_dp4a(const int8_t *in, int8_t *out, const Sizes &s,
                                   cudaStream_t st) {
-  const long long row_bytes = (long long)s.f * s.n * 4;
-  const long long groups = (long long)(s.t / 4) * row_bytes;
-  fmt::unswizzle_kernel<<<fmt::grid_for(groups, 256), 256, 0, st>>>((const uint32_t *)in, out,
-                                                                    groups, row_bytes);
+  const long long row_words = (long long)s.f * s.n;   // t is a multiple of 4 (ntimepipe % 16 == 0)
+  const long long quads = (long long)(s.t / 4) * row_words;
+  fmt::unswizzle_kernel<<<fmt::grid_for(quads, 256), 256, 0, st>>>((const uint4 *)in,
+                                                                   (uint32_t *)out, quads, row_words);
   return cudaGetLastError();
 }
 
