@@ -335,14 +335,8 @@ static dim3 plain_grid(const Sizes &s, int ksplit = 1) {
 // its 8192 sums per block with int64 atomics).  Measured at F=10, T=1024:
 // N=256 155 -> 137 us (2 splits), N=64 60 -> 27 us (4 splits).
 static int plain_splits(const Sizes &s, int tcount) {
-  static int slots = 0;
-  if (!slots) {
-    int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-      return 1;
-    slots = 2 * sms;
-  }
+  const int slots = 2 * current_device_sms();
+  if (!slots) return 1;
   const dim3 g = plain_grid(s);
   const long long blocks = (long long)g.x * g.y;
   long long k = (2LL * slots + blocks - 1) / blocks;

@@ -38,6 +38,8 @@
 // waits (bounded) for its own copies and MMAs, frees its TMEM and returns.
 #include <cudaTypedefs.h>
 
+#include <atomic>
+
 #include "internal.h"
 #include "tc_job.h"
 #include "tc_common.cuh"
@@ -433,25 +435,41 @@ int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
   return r == CUDA_SUCCESS ? 0 : -3;
 }
 
-static int tc_num_sms() {
-  static int num_sms = 0;
-  if (!num_sms) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
-      num_sms = 0;
-      return 0;
-    }
+int current_device_sms() {
+  static std::atomic<int> cache[kDeviceCache];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (dev >= 0 && dev < kDeviceCache) {
+    const int n = cache[dev].load(std::memory_order_relaxed);
+    if (n) return n;
   }
-  return num_sms;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (dev >= 0 && dev < kDeviceCache) cache[dev].store(n, std::memory_order_relaxed);
+  return n;
+}
+
+// Both tcgen05 kernels use more than 48 KB of dynamic shared memory, which a
+// kernel must be allowed on every device it runs on: set it once per device.
+cudaError_t tc_configure_device() {
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < kDeviceCache) ? 1ull << dev : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(tc::xengine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           tc::kSmemBytes);
+  if (e == cudaSuccess) e = tc2_set_smem_attribute();
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+  return e;
 }
 
 cudaError_t tc_check_device() {
   cudaFuncAttributes a;
   cudaError_t e = cudaFuncGetAttributes(&a, tc::xengine_tc_kernel);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(tc::xengine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              tc::kSmemBytes);
+  return tc_configure_device();
 }
 
 int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount, int64_t *state,
@@ -491,14 +509,11 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
                             const TcTuning &tune, int overlap) {
   if (tune.wide) return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap);
-  const int sms = tc_num_sms();
+  const int sms = current_device_sms();
   if (!sms) return cudaErrorInvalidDevice;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(
-        tc::xengine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes);
+  {
+    const cudaError_t e = tc_configure_device();
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   tc::Params p;
   p.single.map = map;
@@ -557,10 +572,9 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
 
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
                             int grid, cudaStream_t st) {
-  const int sms = tc_num_sms();
+  const int sms = current_device_sms();
   if (!sms) return cudaErrorInvalidDevice;
-  cudaError_t e = cudaFuncSetAttribute(tc::xengine_tc_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes);
+  cudaError_t e = tc_configure_device();
   if (e != cudaSuccess) return e;
   if (queue) {
     e = cudaMemsetAsync(queue, 0, sizeof(int), st);

@@ -580,19 +580,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 
 }  // namespace tc2
 
+cudaError_t tc2_set_smem_attribute() {
+  return cudaFuncSetAttribute(tc2::xengine_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              tc2::kSmemBytes);
+}
+
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap) {
-  static int num_sms = 0;
-  static bool configured = false;
-  if (!configured) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(tc2::xengine_tc2_kernel,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, tc2::kSmemBytes);
+  const int num_sms = current_device_sms();
+  if (!num_sms) return cudaErrorInvalidDevice;
+  {
+    const cudaError_t e = tc_configure_device();
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   tc2::Params p;
   Job &j = p.job;
@@ -648,12 +647,9 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
 
 cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
                              int grid, cudaStream_t st, int max_item_steps) {
-  int dev = 0, sms = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tc2::xengine_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tc2::kSmemBytes);
+  const int sms = current_device_sms();
+  if (!sms) return cudaErrorInvalidDevice;
+  cudaError_t e = tc_configure_device();
   if (e != cudaSuccess) return e;
   if (queue) {
     e = cudaMemsetAsync(queue, 0, sizeof(int), st);

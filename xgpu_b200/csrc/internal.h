@@ -88,6 +88,13 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
 int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);
 // 0 if the tensor-core kernel image loads on the current device.
 cudaError_t tc_check_device();
+// Per-device set-up and facts, cached for devices 0 .. kDeviceCache-1 (others are
+// queried or set on every call): the SM count of the current device, and the
+// dynamic shared-memory allowance of both tcgen05 kernels on it.
+constexpr int kDeviceCache = 64;
+int current_device_sms();
+cudaError_t tc_configure_device();
+cudaError_t tc2_set_smem_attribute();
 
 // ---- input conversion, output formatting, synthetic input -----------------
 cudaError_t launch_unpack4(const uint8_t *in, int8_t *out, long long nsamples, cudaStream_t st);
