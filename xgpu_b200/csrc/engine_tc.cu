@@ -36,6 +36,9 @@
 // Every mbarrier wait is bounded; a timeout writes an error code, raises a
 // CTA-wide abort flag so the other roles stop waiting, and the kernel still
 // waits (bounded) for its own copies and MMAs, frees its TMEM and returns.
+// Single-job launches are programmatic (PDL): the prologue overlaps the
+// previous kernel of the stream, and a launch that only adds into sums the
+// previous launch also only adds into runs beside it (see the kernel body).
 #include <cudaTypedefs.h>
 
 #include <atomic>

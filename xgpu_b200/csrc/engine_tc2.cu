@@ -21,6 +21,9 @@
 // "accumulator full" barriers, and the peer's epilogue arrives remotely on the
 // leader's "accumulator empty" barrier.  Every wait is bounded (as in
 // engine_tc.cu); both CTAs meet at a cluster barrier before releasing TMEM.
+// Like engine_tc.cu the kernel is launched programmatically (an adding launch
+// may run beside the previous one), and its epilogue has two schedules, joint
+// and split per warp, chosen by the length of the launch's items.
 #include <cudaTypedefs.h>
 #include <string.h>
 
