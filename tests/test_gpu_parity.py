@@ -416,3 +416,39 @@ def test_long_overlapping_integration_past_int32(xg, oracle_mod, pair):
         for _ in range(3):
             c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
         assert np.array_equal(c.dump(), (73 * one).astype(np.int32))
+
+
+@pytest.mark.parametrize("n,f,t,tune", [(48, 2, 1040, (1, 0, 0)),    # partial block and stage
+                                        (64, 3, 512, (3, 0, 0)),     # time splits
+                                        (128, 2, 2048, (1, 0, 2)),   # stream-K shares
+                                        (96, 1, 256, (1, 0, 1)),     # CTA pairs: pre-pass
+                                        (32, 1, 65536 + 256, (1, 0, 0))])   # three segments
+def test_packed4_tensor_paths(xg, oracle_mod, n, f, t, tune):
+    """Packed 4+4-bit input on the tensor engine, expanded by the pre-pass, with
+    each kernel choice, partial station blocks and stages, and long calls."""
+    packed = oracle_mod.generate(t * f * n * 2, 1, n + t)
+    exact = oracle_mod.xengine_i64(oracle_mod.unpack4(packed), n, f, t)
+    with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor", input_format="packed4") as c:
+        c.tune(*tune)
+        c.set_input(packed)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)     # stores into the cleared buffer
+        c.run(xg.SYNCOP_DUMP)             # adds
+        assert np.array_equal(c.dump_int64(), 2 * exact)
+
+
+def test_packed4_autotune_and_overlapping_device_calls(xg, oracle_mod):
+    """Autotuning a packed context (its input buffers hold one byte per sample;
+    the timing runs on its int8 conversion buffer), then several calls in
+    flight, each converted on the side stream, stay exact."""
+    import torch
+    n, f, t = 256, 4, 1024
+    ps = [oracle_mod.generate(t * f * n * 2, 1, 40 + q) for q in range(3)]
+    ds = [torch.from_numpy(p.view(np.int8)).cuda() for p in ps]
+    torch.cuda.synchronize()
+    one = sum(oracle_mod.xengine_i64(oracle_mod.unpack4(p), n, f, t) for p in ps)
+    with xg.Correlator(n, f, t, engine="tensor", input_format="packed4") as c:
+        c.tune(0)
+        for _ in range(2):
+            for d in ds:
+                c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        assert np.array_equal(c.dump_int64(), 2 * one)

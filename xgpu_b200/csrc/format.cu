@@ -10,6 +10,7 @@
 #include <math.h>
 
 #include "internal.h"
+#include "packed4.cuh"
 
 namespace xgpu {
 
@@ -68,21 +69,13 @@ __global__ void format_kernel(const Params p) {
   }
 }
 
-// Four packed 4+4-bit samples (re high nibble, im low nibble, two's
-// complement) -> eight int8 bytes {re, im} in the same order.  Byte-wise:
-// a nibble v in 0..15 is the signed value (v ^ 8) - 8.
-__device__ __forceinline__ uint2 expand4(uint32_t w) {
-  const uint32_t re = __vsub4(((w >> 4) & 0x0F0F0F0Fu) ^ 0x08080808u, 0x08080808u);
-  const uint32_t im = __vsub4((w & 0x0F0F0F0Fu) ^ 0x08080808u, 0x08080808u);
-  return make_uint2(__byte_perm(re, im, 0x5140), __byte_perm(re, im, 0x7362));
-}
-
 // 16 packed samples per thread: one 16-byte load, two 16-byte stores.
 __global__ void unpack4_kernel(const uint4 *in, uint4 *out, long long nquads) {
   for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nquads;
        u += (long long)gridDim.x * blockDim.x) {
     const uint4 w = in[u];
-    const uint2 a = expand4(w.x), b = expand4(w.y), c = expand4(w.z), d = expand4(w.w);
+    const uint2 a = expand_packed4(w.x), b = expand_packed4(w.y), c = expand_packed4(w.z),
+                d = expand_packed4(w.w);
     out[2 * u] = make_uint4(a.x, a.y, b.x, b.y);
     out[2 * u + 1] = make_uint4(c.x, c.y, d.x, d.y);
   }

@@ -696,16 +696,20 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   XGPU_CHECK(cudaSetDevice(in->device));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
   const Sizes &s = in->sz;
-  // Synthetic input in the first input buffer (its contents are replaced by
-  // the next xgpuCudaXengine anyway) and a scratch integration buffer.
-  XGPU_CHECK(launch_generate(in->d_in[0], (size_t)(2 * s.vec_length), 0, 12345, 16.0, in->s_comp));
+  // Synthetic int8 input where the engine reads it -- the first input buffer
+  // of an int8 context (its contents are replaced by the next call anyway),
+  // the first conversion buffer of the other formats (the input buffers of a
+  // packed context hold only one byte per sample) -- and a scratch
+  // integration buffer.
+  void *tune_in = in->cfg.input_format == XGPU_INPUT_INT8 ? in->d_in[0] : (void *)in->d_conv[0];
+  XGPU_CHECK(launch_generate(tune_in, (size_t)(2 * s.vec_length), 0, 12345, 16.0, in->s_comp));
   void *scratch = nullptr;
   if (cudaMalloc(&scratch, (size_t)s.state_elems * 8) != cudaSuccess) {
     cudaGetLastError();
     return XGPU_OUT_OF_MEMORY;
   }
   CUtensorMap map;
-  if (make_tc_tensor_map(&map, in->d_in[0], s) != 0) {
+  if (make_tc_tensor_map(&map, tune_in, s) != 0) {
     cudaFree(scratch);
     return XGPU_CUDA_ERROR;
   }
