@@ -11,13 +11,17 @@
 // What changes is the data path.  xGPU fetches one sample at a time through
 // textures and swizzled input; here a CTA of 256 threads covers a 32x32
 // station block of one channel, stages 128-byte panels of the natural
-// [t][f][s][p][c] input into shared memory with 16-byte cp.async loads
-// (double buffered), and converts them in shared memory -- to 4-sample
+// [t][f][s][p][c] input into shared memory with TMA (one thread issues each
+// chunk's panels on an mbarrier, double buffered; stations past n and samples
+// past the input are zero-filled), and converts them in shared memory -- to 4-sample
 // words for dp4a (a 4x4 byte transpose with PRMT) or to floats -- in an order
 // that makes the 128-bit shared loads of the compute loop conflict-free.
 // One launch covers a whole time range (not one NTIME_PIPE chunk), and the
 // sums are added to the integration buffer once, at the end.
+#include <atomic>
+
 #include "internal.h"
+#include "tc_common.cuh"
 
 namespace xgpu {
 namespace plain {
@@ -25,19 +29,6 @@ namespace plain {
 constexpr int kBlk = 32;        // stations per block side
 constexpr int kThreads = 256;   // 16 x 16 threads, 2x2 stations each
 constexpr int kRowBytes = kBlk * 4;   // one sample of one panel: 32 stations x 2 pol x re/im
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
-               "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 __device__ __forceinline__ void decode_block(int k, int &rb, int &cb) {
   int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
@@ -53,31 +44,36 @@ __device__ __forceinline__ void decode_block(int k, int &rb, int &cb) {
 __device__ __forceinline__ int slot_of(int s) { return (s & 1) * 16 + (s >> 1); }
 
 struct Params {
-  const int8_t *in;
+  CUtensorMap map;  // the input, boxes of 128 bytes x one chunk of samples
   int n, f;
   int t0, tcount;
   long long nbaseline;
   void *state;
   int overwrite;
-  int per;        // samples per time split (blockIdx.z); == tcount without splits
+  int per;          // samples per time split (blockIdx.z); == tcount without splits
+  int *err;         // receives kErrTimeoutPanel (may be null)
 };
 
-// Issue the cp.async loads of samples [tb, tb+nt) of one panel (32 stations
-// from s0) into raw (nt rows of 128 bytes).  Samples past tend and stations
-// past n are zero-filled.
+// Queue the TMA loads of samples [tb, tb+NT) of the row panel (and, off the
+// diagonal, the column panel) into raw[0] / raw[1], completing on bar.
+// Called by one thread.
 template <int NT>
-__device__ __forceinline__ void load_panel(uint8_t *raw, const Params &p, int f, int s0, int tb,
-                                           int tend) {
-  constexpr int kPieces = NT * (kRowBytes / 16);
-  for (int q = threadIdx.x; q < kPieces; q += kThreads) {
-    const int r = q >> 3, piece = q & 7;
-    const int t = tb + r;
-    const int s = s0 + piece * 4;   // 16 bytes = 4 stations
-    const bool ok = (t < tend) && (s < p.n);
-    const int8_t *src =
-        ok ? p.in + (((long long)t * p.f + f) * p.n + s) * 4 : p.in;
-    cp_async16((uint32_t)__cvta_generic_to_shared(raw + r * kRowBytes + piece * 16), src,
-               ok ? 16 : 0);
+__device__ __forceinline__ void issue_panels(uint8_t (*raw)[NT * kRowBytes], uint32_t bar,
+                                             const Params &p, int f, int rb, int cb, bool diag,
+                                             int tb) {
+  tc::mbar_expect_tx(bar, (diag ? 1 : 2) * NT * kRowBytes);
+  tc::tma_load_3d(tc::smem_u32(raw[0]), &p.map, bar, rb * kRowBytes, f, tb);
+  if (!diag) tc::tma_load_3d(tc::smem_u32(raw[1]), &p.map, bar, cb * kRowBytes, f, tb);
+}
+
+// A panel that never arrived (bounded wait expired): record it and leave
+// without touching the integration buffer, after the other buffer's load (if
+// one is in flight) has landed or its wait has expired too.
+__device__ __forceinline__ void panel_timeout(const Params &p, uint32_t other_bar,
+                                              uint32_t other_parity, bool other_in_flight) {
+  if (threadIdx.x == 0) {
+    if (p.err) atomicExch(p.err, kErrTimeoutPanel);
+    if (other_in_flight) tc::mbar_wait(other_bar, other_parity, nullptr);
   }
 }
 
@@ -111,9 +107,17 @@ __device__ __forceinline__ void to_words(const uint8_t *raw, int4 *words) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const Params p) {
-  __shared__ __align__(16) uint8_t raw[2][2][kRawPanel];
-  __shared__ __align__(16) int4 words[2][kWordPanel / 16];
+// Dynamic shared memory of the dp4a kernel: raw panels [2 buffers][2 panels],
+// converted words [2 panels], two mbarriers, and room to align the panels to
+// 128 bytes (TMA destinations).
+constexpr int kSmemDp4a = 2 * 2 * kRawPanel + 2 * kWordPanel + 16 + 128;
+
+__global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_constant__ Params p) {
+  extern __shared__ __align__(128) uint8_t dsm_raw[];
+  uint8_t *dsm = (uint8_t *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
+  auto raw = (uint8_t(*)[2][kRawPanel])dsm;
+  auto words = (int4(*)[kWordPanel / 16])(dsm + 2 * 2 * kRawPanel);
+  uint64_t *bars = (uint64_t *)(dsm + 2 * 2 * kRawPanel + 2 * kWordPanel);
 
   const int f = blockIdx.y;
   int rb, cb;
@@ -133,22 +137,27 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const Params 
     (&i2[0][0][0][0])[a] = 0;
   }
 
-  load_panel<kTcD>(raw[0][0], p, f, rb * kBlk, tbeg, tend);
-  if (!diag) load_panel<kTcD>(raw[0][1], p, f, cb * kBlk, tbeg, tend);
-  cp_async_commit();
+  const uint32_t bar0 = tc::smem_u32(&bars[0]);
+  if (threadIdx.x == 0) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.map) : "memory");
+    tc::mbar_init(bar0, 1);
+    tc::mbar_init(bar0 + 8, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    issue_panels<kTcD>(raw[0], bar0, p, f, rb, cb, diag, tbeg);
+  }
+  __syncthreads();
 
   for (int ch = 0; ch < nchunks; ++ch) {
     const int buf = ch & 1;
-    if (ch + 1 < nchunks) {
-      const int tb = tbeg + (ch + 1) * kTcD;
-      load_panel<kTcD>(raw[buf ^ 1][0], p, f, rb * kBlk, tb, tend);
-      if (!diag) load_panel<kTcD>(raw[buf ^ 1][1], p, f, cb * kBlk, tb, tend);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+    // Chunk ch+1 goes into the other buffer, free since the end of chunk ch-1.
+    if (threadIdx.x == 0 && ch + 1 < nchunks)
+      issue_panels<kTcD>(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, diag,
+                         tbeg + (ch + 1) * kTcD);
+    const bool got = tc::mbar_wait(bar0 + 8 * buf, (ch >> 1) & 1, nullptr);
+    if (__syncthreads_or(!got)) {
+      panel_timeout(p, bar0 + 8 * (buf ^ 1), ((ch + 1) >> 1) & 1, ch + 1 < nchunks);
+      return;
     }
-    __syncthreads();
     to_words(raw[buf][0], words[0]);
     if (!diag) to_words(raw[buf][1], words[1]);
     __syncthreads();
@@ -226,16 +235,22 @@ __device__ __forceinline__ void to_floats(const uint8_t *raw, float4 *fl) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const Params p) {
-  __shared__ __align__(16) uint8_t raw[2][2][kRawPanelF];
-  __shared__ __align__(16) float4 fl[2][kFloatPanel];
+// Dynamic shared memory of the FP32 kernel: raw panels [2 buffers][2 panels],
+// floats [2 panels], two mbarriers, and room to align the panels to 128 bytes.
+constexpr int kSmemFp32 = 2 * 2 * kRawPanelF + 2 * kFloatPanel * 16 + 16 + 128;
+
+__global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_constant__ Params p) {
+  extern __shared__ __align__(128) uint8_t dsm_raw[];
+  uint8_t *dsm = (uint8_t *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
+  auto raw = (uint8_t(*)[2][kRawPanelF])dsm;
+  auto fl = (float4(*)[kFloatPanel])(dsm + 2 * 2 * kRawPanelF);
+  uint64_t *bars = (uint64_t *)(dsm + 2 * 2 * kRawPanelF + 2 * kFloatPanel * 16);
 
   const int f = blockIdx.y;
   int rb, cb;
   decode_block(blockIdx.x, rb, cb);
   const bool diag = (rb == cb);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int tend = p.t0 + p.tcount;
   const int nchunks = (p.tcount + kTcF - 1) / kTcF;
 
   float sr[2][2][2][2], si[2][2][2][2];
@@ -245,22 +260,27 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const Params p) 
     (&si[0][0][0][0])[a] = 0.f;
   }
 
-  load_panel<kTcF>(raw[0][0], p, f, rb * kBlk, p.t0, tend);
-  if (!diag) load_panel<kTcF>(raw[0][1], p, f, cb * kBlk, p.t0, tend);
-  cp_async_commit();
+  const uint32_t bar0 = tc::smem_u32(&bars[0]);
+  if (threadIdx.x == 0) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.map) : "memory");
+    tc::mbar_init(bar0, 1);
+    tc::mbar_init(bar0 + 8, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    issue_panels<kTcF>(raw[0], bar0, p, f, rb, cb, diag, p.t0);
+  }
+  __syncthreads();
 
   for (int ch = 0; ch < nchunks; ++ch) {
     const int buf = ch & 1;
-    if (ch + 1 < nchunks) {
-      const int tb = p.t0 + (ch + 1) * kTcF;
-      load_panel<kTcF>(raw[buf ^ 1][0], p, f, rb * kBlk, tb, tend);
-      if (!diag) load_panel<kTcF>(raw[buf ^ 1][1], p, f, cb * kBlk, tb, tend);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+    // Chunk ch+1 goes into the other buffer, free since the end of chunk ch-1.
+    if (threadIdx.x == 0 && ch + 1 < nchunks)
+      issue_panels<kTcF>(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, diag,
+                         p.t0 + (ch + 1) * kTcF);
+    const bool got = tc::mbar_wait(bar0 + 8 * buf, (ch >> 1) & 1, nullptr);
+    if (__syncthreads_or(!got)) {
+      panel_timeout(p, bar0 + 8 * (buf ^ 1), ((ch + 1) >> 1) & 1, ch + 1 < nchunks);
+      return;
     }
-    __syncthreads();
     to_floats(raw[buf][0], fl[0]);
     if (!diag) to_floats(raw[buf][1], fl[1]);
     __syncthreads();
@@ -345,8 +365,41 @@ static int plain_splits(const Sizes &s, int tcount) {
   return k < 1 ? 1 : (int)k;
 }
 
+// Both kernels take just over 48 KB of shared memory (the panels plus their
+// mbarriers): allow it once per device.
+static cudaError_t plain_configure_device() {
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < kDeviceCache) ? 1ull << dev : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(plain::xengine_dp4a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           plain::kSmemDp4a);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(plain::xengine_fp32_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, plain::kSmemFp32);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
+
+static int plain_params(plain::Params *p, const int8_t *in, const Sizes &s, int t0, int tcount,
+                        void *state, int overwrite, int per, int rows, int *err) {
+  if (make_panel_map(&p->map, in, s, rows) != 0) return -1;
+  p->n = s.n;
+  p->f = s.f;
+  p->t0 = t0;
+  p->tcount = tcount;
+  p->nbaseline = s.nbaseline;
+  p->state = state;
+  p->overwrite = overwrite;
+  p->per = per;
+  p->err = err;
+  return 0;
+}
+
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
-                              int64_t *state, int overwrite, cudaStream_t st) {
+                              int64_t *state, int overwrite, cudaStream_t st, int *err) {
   const int ks = plain_splits(s, tcount);
   // samples per split: a whole number of 64-sample chunks
   int per = (tcount + ks - 1) / ks;
@@ -356,15 +409,23 @@ cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcou
     cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
     if (e != cudaSuccess) return e;
   }
-  plain::Params p{in, s.n, s.f, t0, tcount, s.nbaseline, state, overwrite, per};
-  plain::xengine_dp4a_kernel<<<plain_grid(s, used), plain::kThreads, 0, st>>>(p);
+  cudaError_t e = plain_configure_device();
+  if (e != cudaSuccess) return e;
+  plain::Params p;
+  if (plain_params(&p, in, s, t0, tcount, state, overwrite, per, plain::kTcD, err) != 0)
+    return cudaErrorInvalidValue;
+  plain::xengine_dp4a_kernel<<<plain_grid(s, used), plain::kThreads, plain::kSmemDp4a, st>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount, float *state,
-                              int overwrite, cudaStream_t st) {
-  plain::Params p{in, s.n, s.f, t0, tcount, s.nbaseline, state, overwrite, tcount};
-  plain::xengine_fp32_kernel<<<plain_grid(s), plain::kThreads, 0, st>>>(p);
+                              int overwrite, cudaStream_t st, int *err) {
+  cudaError_t e = plain_configure_device();
+  if (e != cudaSuccess) return e;
+  plain::Params p;
+  if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err) != 0)
+    return cudaErrorInvalidValue;
+  plain::xengine_fp32_kernel<<<plain_grid(s), plain::kThreads, plain::kSmemFp32, st>>>(p);
   return cudaGetLastError();
 }
 

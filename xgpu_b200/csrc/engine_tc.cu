@@ -415,7 +415,8 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
 
 }  // namespace tc
 
-int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
+// cuTensorMapEncodeTiled, resolved once through the runtime.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult q;
@@ -423,19 +424,35 @@ int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
             cudaSuccess ||
         q != cudaDriverEntryPointSuccess || !fn)
-      return -1;
+      return nullptr;
     encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
   }
+  return encode;
+}
+
+// {x: 4n bytes, y: f, z: t} over [t][f][s][p][c] int8 input; boxes of
+// 128 bytes (32 stations) x `rows` samples.
+static int input_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int rows,
+                     CUtensorMapSwizzle swizzle) {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return -1;
   if (((uintptr_t)dev_in & 15) != 0) return -2;
   cuuint64_t dims[3] = {(cuuint64_t)4 * s.n, (cuuint64_t)s.f, (cuuint64_t)s.t};
   cuuint64_t strides[2] = {(cuuint64_t)4 * s.n, (cuuint64_t)4 * s.n * s.f};
-  cuuint32_t box[3] = {(cuuint32_t)tc::kTile, 1, (cuuint32_t)tc::kKt};
+  cuuint32_t box[3] = {(cuuint32_t)tc::kTile, 1, (cuuint32_t)rows};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(dev_in), dims,
-                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : -3;
+}
+
+int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
+  return input_map(map, dev_in, s, tc::kKt, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+int make_panel_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int rows) {
+  return input_map(map, dev_in, s, rows, CU_TENSOR_MAP_SWIZZLE_NONE);
 }
 
 int current_device_sms() {

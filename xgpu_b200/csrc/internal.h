@@ -25,6 +25,7 @@ enum DeviceError : int {
   kErrTimeoutProducer = 1,   // TMA producer gave up waiting for a free stage
   kErrTimeoutMma = 2,        // MMA issuer gave up waiting for a loaded stage
   kErrTimeoutDrain = 3,      // epilogue gave up waiting for the accumulator
+  kErrTimeoutPanel = 4,      // plain engine gave up waiting for an input panel
 };
 
 struct Sizes {
@@ -48,10 +49,12 @@ Sizes make_sizes(const XGPUConfig &cfg);
 // state[f][k][p1][p2][re,im], k = i(i+1)/2 + j, i >= j.  overwrite != 0
 // stores instead of adding (the buffer is known to be zero).
 
+// The plain engines load their input panels with TMA; err (may be null)
+// receives kErrTimeoutPanel if a panel never arrives.
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
-                              int64_t *state, int overwrite, cudaStream_t st);
+                              int64_t *state, int overwrite, cudaStream_t st, int *err = nullptr);
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount,
-                              float *state, int overwrite, cudaStream_t st);
+                              float *state, int overwrite, cudaStream_t st, int *err = nullptr);
 
 // Tensor-core engine.  The tensor map describes `in` (see make_tc_tensor_map).
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
@@ -86,6 +89,9 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
 // Encodes the 3-D tensor map {x: 4n bytes, y: f, z: t} over a device input
 // buffer.  Returns 0 on success.
 int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);
+// The same map with unswizzled boxes of 128 bytes x `rows` samples (the plain
+// engines' panels).
+int make_panel_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int rows);
 // 0 if the tensor-core kernel image loads on the current device.
 cudaError_t tc_check_device();
 // Per-device set-up and facts, cached for devices 0 .. kDeviceCache-1 (others are

@@ -401,7 +401,7 @@ extern "C" int xgpuServeRun(const XGPUServeJob *jobs, int njobs, const XGPUServe
             const char *x = pool[a.bucket] + block_offset(j.seed, b);
             if (plain) {
               SCHECK(launch_plain_dp4a((const int8_t *)x, a.s, 0, a.s.t, (int64_t *)a.state,
-                                       b == 0, s_step));
+                                       b == 0, s_step, d_err));
             } else {
               Job &jb = tab[nent++];
               if (tc_fill_job(&jb, x, a.s, 0, a.s.t, (int64_t *)a.state,
