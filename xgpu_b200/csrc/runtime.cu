@@ -727,7 +727,7 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   struct Cand {
     int ksplit, grid, wide, streamk;
   };
-  Cand cands[24];
+  Cand cands[32];
   int ncand = 0;
   const int splits[] = {1, 2, 3, 4, 6, 8};
   for (int wide = 0; wide < 2; ++wide)
@@ -737,8 +737,7 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
     for (int d : {2, 4, 6, 8}) cands[ncand++] = {1, sms / d, 0, 0};
     cands[ncand++] = {2, sms / 2, 0, 0};
     cands[ncand++] = {2, sms / 4, 0, 0};
-    cands[ncand++] = {1, sms / 2, 1, 0};
-    cands[ncand++] = {1, sms / 4, 1, 0};
+    for (int d : {2, 4, 6, 8}) cands[ncand++] = {1, sms / d, 1, 0};
   }
   int rc = XGPU_OK;
   for (int ci = 0; ci < ncand; ++ci) {
