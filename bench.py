@@ -347,9 +347,9 @@ def bench_config3(xg, torch, device, blocks=64):
     linearity: 64 blocks alternating A, B must equal 32 x (A + B)."""
     out = {"nstation": N3, "nfrequency": F3, "ntime": T3, "blocks": blocks}
     for fmt, kind, sig in (("packed4", 1, 0.0), ("int8", 0, 40.0)):
-        # The context's own streams (packed input is expanded on a side stream,
-        # overlapping the previous block's correlation); timed by the host
-        # around a synchronised 64-block run (hundreds of ms).
+        # The context's own streams (packed input is expanded on a side stream
+        # before each block's correlation); timed by the host around a
+        # synchronised 64-block run (hundreds of ms).
         c = xg.Correlator(N3, F3, T3, ntimepipe=128, engine="tensor", input_format=fmt,
                           device=device)
         c.tune(1, 0, 1)

@@ -63,9 +63,11 @@ struct Internal {
   bool int_state = true;  // int64 buffer (integer engines) or float (FP32)
 
   void *d_in[2] = {nullptr, nullptr};  // one call's input, as supplied
-  // Packed 4+4-bit and DP4A-swizzled input is converted to int8
+  // Packed 4+4-bit, DP4A-swizzled and block-32 input is converted to int8
   // [t][f][s][p][c] on its own stream into one of two buffers, so the
-  // conversion of call k+1 runs under the engine of call k.
+  // conversion of call k+1 is queued without waiting for the engine of call
+  // k (measured: the two kernels seldom share the SMs, so a converted call
+  // costs its conversion plus its engine launch).
   int8_t *d_conv[2] = {nullptr, nullptr};
   cudaStream_t s_conv = nullptr;
   cudaEvent_t conv_done[2] = {nullptr, nullptr};
