@@ -83,3 +83,45 @@ def test_random_configuration(xg, oracle_mod, case):
             # float sums of integers are exact below 2^24
             assert np.abs(exact).max() < 2**24
             assert np.array_equal(got, exact.astype(np.float32)), case
+
+
+def draw_batches():
+    rng = np.random.default_rng(SEED + 1)
+    out = []
+    for q in range(6):
+        njobs = int(rng.integers(3, 16))
+        jobs = []
+        for k in range(njobs):
+            n = int(rng.choice([16, 32, 48, 80, 128, 176, 256, 384]))
+            f = int(rng.integers(1, 9))
+            t = int(256 * rng.integers(1, 9)) if rng.integers(0, 2) else int(16 * rng.integers(1, 40))
+            jobs.append((n, f, t, int(rng.integers(0, 2))))
+        flags = (bool(rng.integers(0, 2)), bool(rng.integers(0, 2)), bool(rng.integers(0, 2)))
+        runs = int(rng.integers(1, 4))
+        out.append((q, jobs, flags, runs))
+    return out
+
+
+@pytest.mark.parametrize("batch", draw_batches(), ids=lambda b: f"batch{b[0]}")
+def test_random_batch(xg, oracle_mod, batch):
+    """A random batch of uneven subarrays (some accumulating, some replacing
+    their buffer each run), with random autotune / graph / CTA-pair flags, run
+    one to three times: every job's int64 buffer equals the oracle."""
+    import torch
+    q, shapes, (autotune, graph, pair), runs = batch
+    jobs, keep = [], []
+    for k, (n, f, t, acc) in enumerate(shapes):
+        x = oracle_mod.gaussian_input(n, f, t, seed=7000 + 100 * q + k, sigma=float(4 + 7 * k % 40))
+        xd = torch.from_numpy(x).cuda()
+        st = torch.zeros(f * n * (n + 1) // 2 * 8, dtype=torch.int64, device="cuda")
+        jobs.append({"input": xd.data_ptr(), "state": st.data_ptr(), "nstation": n,
+                     "nfrequency": f, "ntime": t, "accumulate": acc})
+        keep.append((x, xd, st, n, f, t, acc))
+    torch.cuda.synchronize()
+    with xg.Batch(jobs, autotune=autotune, graph=graph, pair=pair) as b:
+        for _ in range(runs):
+            b.run()
+        b.sync()
+    for x, xd, st, n, f, t, acc in keep:
+        want = (runs if acc else 1) * oracle_mod.xengine_i64(x, n, f, t)
+        assert np.array_equal(st.cpu().numpy(), want), (n, f, t, acc)
