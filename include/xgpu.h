@@ -314,8 +314,8 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);
 int xgpuTuning(XGPUContext *context, int *ksplit, int *grid, int *pair);
 
 /* Extension for testing a caller's error handling.  While enabled, the
- * tensor-core engine of this context issues no input loads, so its bounded
- * device waits expire (about 2 s per launch) instead of completing: the next
+ * engine of this context (tensor-core or plain) issues no input loads, so its
+ * bounded device waits expire (about 2 s per launch) instead of completing: the next
  * synchronising call returns XGPU_CUDA_ERROR, the integration in progress is
  * invalid, and once disabled the context works normally (clear it first).
  * Nothing faults or hangs. */

@@ -1,8 +1,8 @@
 """Failure detection without a GPU fault.
 
-Every wait of the tensor-core kernels is bounded (about 2 s); when one
-expires the kernel records an error code, the other roles stop, TMEM is
-released and the kernel returns.  xgpuInjectTimeout makes the engine withhold
+Every wait of the tensor-core and plain kernels is bounded (about 2 s); when
+one expires the kernel records an error code, the other roles stop, TMEM (if
+any) is released and the kernel returns without touching the integration.  xgpuInjectTimeout makes the engine withhold
 its input loads so the waits expire on purpose (a flag nothing sets); the
 host must report XGPU_CUDA_ERROR and the context must keep working."""
 import ctypes
@@ -29,3 +29,23 @@ def test_expired_device_wait_is_reported_and_recoverable(xg, oracle_mod, pair):
         c.run(xg.SYNCOP_DUMP)
         got = c.dump_int64()
     assert np.array_equal(got, oracle_mod.xengine_i64(x, n, f, t))
+
+
+@pytest.mark.parametrize("compute", ["int8", "fp32"])
+def test_plain_engine_expired_wait_is_reported_and_recoverable(xg, oracle_mod, compute):
+    """The plain engines' panel waits (TMA on mbarriers) expire the same way."""
+    n, f, t = 64, 2, 512
+    x = oracle_mod.gaussian_input(n, f, t, seed=6)
+    out = "int32" if compute == "int8" else "float32"
+    with xg.Correlator(n, f, t, engine="plain", compute=compute, output=out) as c:
+        c.set_input(x)
+        assert xg.lib().xgpuInjectTimeout(ctypes.byref(c.ctx), 1) == 0
+        with pytest.raises(xg.XGPUError) as err:
+            c.run(xg.SYNCOP_SYNC_COMPUTE)
+        assert err.value.code == xg.XGPU_CUDA_ERROR
+        assert xg.lib().xgpuInjectTimeout(ctypes.byref(c.ctx), 0) == 0
+        c.clear()
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2].copy()
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    assert np.array_equal(got, exact.astype(got.dtype))

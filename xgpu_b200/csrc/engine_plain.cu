@@ -52,6 +52,7 @@ struct Params {
   int overwrite;
   int per;          // samples per time split (blockIdx.z); == tcount without splits
   int *err;         // receives kErrTimeoutPanel (may be null)
+  int stall;        // test switch: issue no panel loads (the waits on them expire)
 };
 
 // Queue the TMA loads of samples [tb, tb+NT) of the row panel (and, off the
@@ -61,6 +62,7 @@ template <int NT>
 __device__ __forceinline__ void issue_panels(uint8_t (*raw)[NT * kRowBytes], uint32_t bar,
                                              const Params &p, int f, int rb, int cb, bool diag,
                                              int tb) {
+  if (p.stall) return;
   tc::mbar_expect_tx(bar, (diag ? 1 : 2) * NT * kRowBytes);
   tc::tma_load_3d(tc::smem_u32(raw[0]), &p.map, bar, rb * kRowBytes, f, tb);
   if (!diag) tc::tma_load_3d(tc::smem_u32(raw[1]), &p.map, bar, cb * kRowBytes, f, tb);
@@ -73,7 +75,7 @@ __device__ __forceinline__ void panel_timeout(const Params &p, uint32_t other_ba
                                               uint32_t other_parity, bool other_in_flight) {
   if (threadIdx.x == 0) {
     if (p.err) atomicExch(p.err, kErrTimeoutPanel);
-    if (other_in_flight) tc::mbar_wait(other_bar, other_parity, nullptr);
+    if (other_in_flight && !p.stall) tc::mbar_wait(other_bar, other_parity, nullptr);
   }
 }
 
@@ -384,7 +386,7 @@ static cudaError_t plain_configure_device() {
 }
 
 static int plain_params(plain::Params *p, const int8_t *in, const Sizes &s, int t0, int tcount,
-                        void *state, int overwrite, int per, int rows, int *err) {
+                        void *state, int overwrite, int per, int rows, int *err, int stall) {
   if (make_panel_map(&p->map, in, s, rows) != 0) return -1;
   p->n = s.n;
   p->f = s.f;
@@ -395,11 +397,13 @@ static int plain_params(plain::Params *p, const int8_t *in, const Sizes &s, int 
   p->overwrite = overwrite;
   p->per = per;
   p->err = err;
+  p->stall = stall;
   return 0;
 }
 
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
-                              int64_t *state, int overwrite, cudaStream_t st, int *err) {
+                              int64_t *state, int overwrite, cudaStream_t st, int *err,
+                              int stall) {
   const int ks = plain_splits(s, tcount);
   // samples per split: a whole number of 64-sample chunks
   int per = (tcount + ks - 1) / ks;
@@ -412,18 +416,18 @@ cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcou
   cudaError_t e = plain_configure_device();
   if (e != cudaSuccess) return e;
   plain::Params p;
-  if (plain_params(&p, in, s, t0, tcount, state, overwrite, per, plain::kTcD, err) != 0)
+  if (plain_params(&p, in, s, t0, tcount, state, overwrite, per, plain::kTcD, err, stall) != 0)
     return cudaErrorInvalidValue;
   plain::xengine_dp4a_kernel<<<plain_grid(s, used), plain::kThreads, plain::kSmemDp4a, st>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount, float *state,
-                              int overwrite, cudaStream_t st, int *err) {
+                              int overwrite, cudaStream_t st, int *err, int stall) {
   cudaError_t e = plain_configure_device();
   if (e != cudaSuccess) return e;
   plain::Params p;
-  if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err) != 0)
+  if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err, stall) != 0)
     return cudaErrorInvalidValue;
   plain::xengine_fp32_kernel<<<plain_grid(s), plain::kThreads, plain::kSmemFp32, st>>>(p);
   return cudaGetLastError();

@@ -50,11 +50,14 @@ Sizes make_sizes(const XGPUConfig &cfg);
 // stores instead of adding (the buffer is known to be zero).
 
 // The plain engines load their input panels with TMA; err (may be null)
-// receives kErrTimeoutPanel if a panel never arrives.
+// receives kErrTimeoutPanel if a panel never arrives.  stall (a test switch)
+// withholds the loads so that happens.
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
-                              int64_t *state, int overwrite, cudaStream_t st, int *err = nullptr);
+                              int64_t *state, int overwrite, cudaStream_t st, int *err = nullptr,
+                              int stall = 0);
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount,
-                              float *state, int overwrite, cudaStream_t st, int *err = nullptr);
+                              float *state, int overwrite, cudaStream_t st, int *err = nullptr,
+                              int stall = 0);
 
 // Tensor-core engine.  The tensor map describes `in` (see make_tc_tensor_map).
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount,

@@ -270,12 +270,13 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   }
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
-    XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err));
+    XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
+                                 in->tune.stall));
   } else if (in->cfg.engine == XGPU_ENGINE_PLAIN) {
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
       XGPU_CHECK(launch_plain_dp4a(x, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
-                                   in->s_comp, in->d_err));
+                                   in->s_comp, in->d_err, in->tune.stall));
     }
   } else {
     const CUtensorMap *map = tensor_map(in, x);
