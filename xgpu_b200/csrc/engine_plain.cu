@@ -53,6 +53,7 @@ struct Params {
   int per;          // samples per time split (blockIdx.z); == tcount without splits
   int *err;         // receives kErrTimeoutPanel (may be null)
   int stall;        // test switch: issue no panel loads (the waits on them expire)
+  int f0;           // first channel (blockIdx.y counts from it)
 };
 
 // Queue the TMA loads of samples [tb, tb+NT) of the row panel (and, off the
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
   auto words = (int4(*)[kWordPanel / 16])(dsm + 2 * 2 * kRawPanel);
   uint64_t *bars = (uint64_t *)(dsm + 2 * 2 * kRawPanel + 2 * kWordPanel);
 
-  const int f = blockIdx.y;
+  const int f = p.f0 + (int)blockIdx.y;
   int rb, cb;
   decode_block(blockIdx.x, rb, cb);
   const bool diag = (rb == cb);
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
   auto fl = (float4(*)[kFloatPanel])(dsm + 2 * 2 * kRawPanelF);
   uint64_t *bars = (uint64_t *)(dsm + 2 * 2 * kRawPanelF + 2 * kFloatPanel * 16);
 
-  const int f = blockIdx.y;
+  const int f = p.f0 + (int)blockIdx.y;
   int rb, cb;
   decode_block(blockIdx.x, rb, cb);
   const bool diag = (rb == cb);
@@ -344,9 +345,9 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
 
 }  // namespace plain
 
-static dim3 plain_grid(const Sizes &s, int ksplit = 1) {
+static dim3 plain_grid(const Sizes &s, int fcount, int ksplit = 1) {
   const int nb = (s.n + plain::kBlk - 1) / plain::kBlk;
-  return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)s.f, (unsigned)ksplit);
+  return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)fcount, (unsigned)ksplit);
 }
 
 // Time splits for the dp4a kernel.  With fewer 32x32-station blocks than two
@@ -356,10 +357,10 @@ static dim3 plain_grid(const Sizes &s, int ksplit = 1) {
 // keeping at least 256 samples per split and at most 8 splits (each split adds
 // its 8192 sums per block with int64 atomics).  Measured at F=10, T=1024:
 // N=256 155 -> 137 us (2 splits), N=64 60 -> 27 us (4 splits).
-static int plain_splits(const Sizes &s, int tcount) {
+static int plain_splits(const Sizes &s, int fcount, int tcount) {
   const int slots = 2 * current_device_sms();
   if (!slots) return 1;
-  const dim3 g = plain_grid(s);
+  const dim3 g = plain_grid(s, fcount);
   const long long blocks = (long long)g.x * g.y;
   long long k = (2LL * slots + blocks - 1) / blocks;
   if (k > tcount / 256) k = tcount / 256;
@@ -386,7 +387,8 @@ static cudaError_t plain_configure_device() {
 }
 
 static int plain_params(plain::Params *p, const int8_t *in, const Sizes &s, int t0, int tcount,
-                        void *state, int overwrite, int per, int rows, int *err, int stall) {
+                        void *state, int overwrite, int per, int rows, int *err, int stall,
+                        int f0) {
   if (make_panel_map(&p->map, in, s, rows) != 0) return -1;
   p->n = s.n;
   p->f = s.f;
@@ -398,38 +400,48 @@ static int plain_params(plain::Params *p, const int8_t *in, const Sizes &s, int 
   p->per = per;
   p->err = err;
   p->stall = stall;
+  p->f0 = f0;
   return 0;
 }
 
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
                               int64_t *state, int overwrite, cudaStream_t st, int *err,
-                              int stall) {
-  const int ks = plain_splits(s, tcount);
+                              int stall, int f0, int fcount) {
+  if (fcount < 0) fcount = s.f - f0;
+  if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
+  const int ks = plain_splits(s, fcount, tcount);
   // samples per split: a whole number of 64-sample chunks
   int per = (tcount + ks - 1) / ks;
   per = (per + plain::kTcD - 1) / plain::kTcD * plain::kTcD;
   const int used = (tcount + per - 1) / per;
-  if (used > 1 && overwrite) {
-    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
+  if (used > 1 && overwrite) {   // the splits add: clear the channel range first
+    const size_t per_channel = (size_t)s.state_elems / s.f;
+    cudaError_t e = cudaMemsetAsync(state + (size_t)f0 * per_channel, 0,
+                                    (size_t)fcount * per_channel * 8, st);
     if (e != cudaSuccess) return e;
   }
   cudaError_t e = plain_configure_device();
   if (e != cudaSuccess) return e;
   plain::Params p;
-  if (plain_params(&p, in, s, t0, tcount, state, overwrite, per, plain::kTcD, err, stall) != 0)
+  if (plain_params(&p, in, s, t0, tcount, state, overwrite, per, plain::kTcD, err, stall, f0) != 0)
     return cudaErrorInvalidValue;
-  plain::xengine_dp4a_kernel<<<plain_grid(s, used), plain::kThreads, plain::kSmemDp4a, st>>>(p);
+  plain::xengine_dp4a_kernel<<<plain_grid(s, fcount, used), plain::kThreads, plain::kSmemDp4a,
+                               st>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount, float *state,
-                              int overwrite, cudaStream_t st, int *err, int stall) {
+                              int overwrite, cudaStream_t st, int *err, int stall, int f0,
+                              int fcount) {
+  if (fcount < 0) fcount = s.f - f0;
+  if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   cudaError_t e = plain_configure_device();
   if (e != cudaSuccess) return e;
   plain::Params p;
-  if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err, stall) != 0)
+  if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err, stall,
+                   f0) != 0)
     return cudaErrorInvalidValue;
-  plain::xengine_fp32_kernel<<<plain_grid(s), plain::kThreads, plain::kSmemFp32, st>>>(p);
+  plain::xengine_fp32_kernel<<<plain_grid(s, fcount), plain::kThreads, plain::kSmemFp32, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -102,7 +102,7 @@ __device__ __forceinline__ Item decode_job(const Job &j, int u) {
   const int k = v % j.npairs;          // tile within the channel
   const int rest = v / j.npairs;
   const int split = rest % j.ksplit;
-  it.f = rest / j.ksplit;
+  it.f = j.f0 + rest / j.ksplit;
   int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
   while (r * (r + 1) / 2 > k) --r;
   while ((r + 1) * (r + 2) / 2 <= k) ++r;
@@ -508,6 +508,7 @@ int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount
   job->nbaseline = s.nbaseline;
   job->n = s.n;
   job->f = s.f;
+  job->f0 = 0;
   job->t0 = t0;
   job->total_steps = total_steps;
   job->steps_per_split = per;
@@ -527,8 +528,11 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune, int overlap) {
-  if (tune.wide) return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap);
+                            const TcTuning &tune, int overlap, int f0, int fcount) {
+  if (fcount < 0) fcount = s.f - f0;
+  if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
+  if (tune.wide)
+    return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap, f0, fcount);
   const int sms = current_device_sms();
   if (!sms) return cudaErrorInvalidDevice;
   {
@@ -545,23 +549,26 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
   int ksplit = tune.ksplit < 1 ? 1 : (tune.ksplit > total_steps ? total_steps : tune.ksplit);
   const int per = (total_steps + ksplit - 1) / ksplit;
   ksplit = (total_steps + per - 1) / per;
-  if ((long long)s.f * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
+  if ((long long)fcount * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
   // Split items of one tile all add into the buffer: a zero buffer must be
-  // cleared first when it would otherwise be stored into.
+  // cleared first (its channel range) when it would otherwise be stored into.
   if (overwrite && ksplit > 1) {
-    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
+    const size_t per_channel = (size_t)s.state_elems / s.f;   // int64 words
+    cudaError_t e = cudaMemsetAsync(state + (size_t)f0 * per_channel, 0,
+                                    (size_t)fcount * per_channel * 8, st);
     if (e != cudaSuccess) return e;
   }
   j.state = state;
   j.nbaseline = s.nbaseline;
   j.n = s.n;
-  j.f = s.f;
+  j.f = fcount;
+  j.f0 = f0;
   j.t0 = t0;
   j.total_steps = total_steps;
   j.steps_per_split = per;
   j.ksplit = ksplit;
   j.npairs = (int)npairs;
-  j.items = (int)(s.f * npairs * ksplit);
+  j.items = (int)(fcount * npairs * ksplit);
   j.item_begin = 0;
   j.store = (overwrite && ksplit == 1) ? 1 : 0;
   p.jobs = nullptr;

@@ -107,7 +107,7 @@ __device__ __forceinline__ Item decode_job(const Job &j, int u) {
   const int k = v % j.npairs;
   const int rest = v / j.npairs;
   const int split = rest % j.ksplit;
-  it.f = rest / j.ksplit;
+  it.f = j.f0 + rest / j.ksplit;
   int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
   while (r * (r + 1) / 2 > k) --r;
   while ((r + 1) * (r + 2) / 2 <= k) ++r;
@@ -589,7 +589,10 @@ cudaError_t tc2_set_smem_attribute() {
 }
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
-                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap) {
+                       int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap,
+                       int f0, int fcount) {
+  if (fcount < 0) fcount = s.f - f0;
+  if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   const int num_sms = current_device_sms();
   if (!num_sms) return cudaErrorInvalidDevice;
   {
@@ -605,21 +608,24 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   int ksplit = tune.ksplit < 1 ? 1 : (tune.ksplit > total_steps ? total_steps : tune.ksplit);
   const int per = (total_steps + ksplit - 1) / ksplit;
   ksplit = (total_steps + per - 1) / per;
-  if ((long long)s.f * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
+  if ((long long)fcount * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
   if (overwrite && ksplit > 1) {
-    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)s.state_elems * 8, st);
+    const size_t per_channel = (size_t)s.state_elems / s.f;   // int64 words
+    cudaError_t e = cudaMemsetAsync(state + (size_t)f0 * per_channel, 0,
+                                    (size_t)fcount * per_channel * 8, st);
     if (e != cudaSuccess) return e;
   }
   j.state = state;
   j.nbaseline = s.nbaseline;
   j.n = s.n;
-  j.f = s.f;
+  j.f = fcount;
+  j.f0 = f0;
   j.t0 = t0;
   j.total_steps = total_steps;
   j.steps_per_split = per;
   j.ksplit = ksplit;
   j.npairs = (int)npairs;
-  j.items = (int)(s.f * npairs * ksplit);
+  j.items = (int)(fcount * npairs * ksplit);
   j.item_begin = 0;
   j.store = (overwrite && ksplit == 1) ? 1 : 0;
   p.jobs = nullptr;

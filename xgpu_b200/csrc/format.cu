@@ -23,6 +23,7 @@ struct Params {
   long long nbaseline, mat_length;
   int order, out_type;
   uint32_t *out;  // matLength Complex = 2*matLength 32-bit words
+  long long u0, u1;   // the (channel, baseline, product) range formatted
 };
 
 __device__ __forceinline__ uint32_t convert(const void *state, int is_float, long long idx,
@@ -39,8 +40,7 @@ __device__ __forceinline__ uint32_t convert(const void *state, int is_float, lon
 
 // One thread per (channel, baseline, polarisation product).
 __global__ void format_kernel(const Params p) {
-  const long long total = (long long)p.f * p.nbaseline * 4;
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total;
+  for (long long u = p.u0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; u < p.u1;
        u += (long long)gridDim.x * blockDim.x) {
     const int pp = (int)(u & 3);
     const long long fk = u >> 2;
@@ -184,15 +184,23 @@ static unsigned grid_for(long long work, int threads) {
 }  // namespace fmt
 
 cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s, int order,
-                          int out_type, void *out, cudaStream_t st) {
+                          int out_type, void *out, cudaStream_t st, int f0, int fcount) {
+  if (fcount < 0) fcount = s.f - f0;
+  if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   if (order == REGISTER_TILE_TRIANGULAR_ORDER) {
-    // Slots that hold no baseline (kernel.cuh:65-71) stay zero.
-    cudaError_t e = cudaMemsetAsync(out, 0, (size_t)s.mat_length * 8, st);
-    if (e != cudaSuccess) return e;
+    // Slots that hold no baseline (kernel.cuh:65-71) stay zero: clear the
+    // channel range's words in both planes.
+    const long long per = s.mat_length / s.f;   // 32-bit words per channel and plane
+    for (int plane = 0; plane < 2; ++plane) {
+      cudaError_t e = cudaMemsetAsync((uint32_t *)out + plane * s.mat_length + f0 * per, 0,
+                                      (size_t)(fcount * per) * 4, st);
+      if (e != cudaSuccess) return e;
+    }
   }
+  const long long per_ch = s.nbaseline * 4;
   fmt::Params p{state, state_is_float, s.n, s.f, s.nbaseline, s.mat_length, order, out_type,
-                (uint32_t *)out};
-  const long long work = (long long)s.f * s.nbaseline * 4;
+                (uint32_t *)out, f0 * per_ch, (f0 + fcount) * per_ch};
+  const long long work = fcount * per_ch;
   fmt::format_kernel<<<fmt::grid_for(work, 256), 256, 0, st>>>(p);
   return cudaGetLastError();
 }

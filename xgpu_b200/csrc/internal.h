@@ -54,10 +54,10 @@ Sizes make_sizes(const XGPUConfig &cfg);
 // withholds the loads so that happens.
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
                               int64_t *state, int overwrite, cudaStream_t st, int *err = nullptr,
-                              int stall = 0);
+                              int stall = 0, int f0 = 0, int fcount = -1);
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount,
                               float *state, int overwrite, cudaStream_t st, int *err = nullptr,
-                              int stall = 0);
+                              int stall = 0, int f0 = 0, int fcount = -1);
 
 // Tensor-core engine.  The tensor map describes `in` (see make_tc_tensor_map).
 cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
@@ -67,14 +67,16 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 // an engine launch of the same integration that does not store (only adds)
 // and that nothing this launch reads was written after it was queued: then,
 // unless this launch stores, the two run side by side, their reduce-adds
-// commuting.
+// commuting.  Channels [f0, f0 + fcount) of the input and buffer are
+// correlated (fcount < 0: through the last channel); an overwrite stores into,
+// or clears, that channel range only.
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune, int overlap);
+                            const TcTuning &tune, int overlap, int f0 = 0, int fcount = -1);
 // The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune,
-                       int overlap);
+                       int overlap, int f0 = 0, int fcount = -1);
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -110,8 +112,11 @@ cudaError_t launch_unpack4(const uint8_t *in, int8_t *out, long long nsamples, c
 cudaError_t launch_unswizzle_dp4a(const int8_t *in, int8_t *out, const Sizes &s, cudaStream_t st);
 cudaError_t launch_unblock32(const int8_t *in, int8_t *out, long long nbytes, cudaStream_t st);
 // state (int64 or float) -> Complex words in `order` of type out_type.
+// Channels [f0, f0 + fcount) of the buffer into `out` in the requested order
+// (fcount < 0: through the last channel); other channels' words are untouched.
 cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s, int order,
-                          int out_type, void *out, cudaStream_t st);
+                          int out_type, void *out, cudaStream_t st, int f0 = 0,
+                          int fcount = -1);
 cudaError_t launch_generate(void *out, size_t nbytes, int kind, unsigned long long seed,
                             double sigma, cudaStream_t st);
 

@@ -56,6 +56,11 @@ using namespace xgpu;
 
 namespace {
 
+// Channel groups of a dumping call with host buffers (see the note at
+// dump_call_grouped): at most this many, each at least kGroupMinBytes of input.
+constexpr int kMaxGroups = 8;
+constexpr long long kGroupMinBytes = 1 << 20;
+
 struct Internal {
   int device = 0;
   XGPUConfig cfg{};
@@ -82,6 +87,12 @@ struct Internal {
 
   cudaStream_t s_copy = nullptr, s_comp = nullptr;
   cudaStream_t s_own = nullptr;  // the context's own compute stream
+  // A dumping call over host buffers moves its channels in groups: group k+1
+  // goes host-to-device while group k's results go device-to-host on s_dump
+  // (the two directions' copy engines run at once).
+  cudaStream_t s_dump = nullptr;
+  cudaEvent_t group_in[kMaxGroups] = {};    // a group's input is on the device
+  cudaEvent_t group_out[kMaxGroups] = {};   // a group's sums (or formatted results) are ready
   cudaEvent_t copy_done[2] = {nullptr, nullptr};
   cudaEvent_t comp_done[2] = {nullptr, nullptr};
   int cur = 0;
@@ -180,6 +191,14 @@ int free_device(Internal *in) {
   }
   if (in->s_copy) cudaStreamDestroy(in->s_copy);
   if (in->s_own) cudaStreamDestroy(in->s_own);
+  if (in->s_dump) {
+    cudaStreamSynchronize(in->s_dump);
+    cudaStreamDestroy(in->s_dump);
+  }
+  for (int k = 0; k < kMaxGroups; ++k) {
+    if (in->group_in[k]) cudaEventDestroy(in->group_in[k]);
+    if (in->group_out[k]) cudaEventDestroy(in->group_out[k]);
+  }
   for (int k = 0; k < 2; ++k) {
     if (in->d_conv[k]) cudaFree(in->d_conv[k]);
     if (in->conv_done[k]) cudaEventDestroy(in->conv_done[k]);
@@ -232,6 +251,39 @@ const CUtensorMap *tensor_map(Internal *in, const void *ptr) {
   return &in->maps[slot].map;
 }
 
+// Queue the engine over channels [f0, f0 + fcount) of int8 input x on s_comp,
+// in time segments; the first segment stores when the buffer is known to be
+// zero.  *tail: in, the launch may overlap the adding launch before it; out,
+// the last launch queued only added.
+int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail) {
+  const Sizes &s = in->sz;
+  const int ow = in->state_zero ? 1 : 0;
+  if (!in->int_state) {
+    XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
+                                 in->tune.stall, f0, fcount));
+  } else if (in->cfg.engine == XGPU_ENGINE_PLAIN) {
+    for (int t0 = 0; t0 < s.t; t0 += kSegment) {
+      const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
+      XGPU_CHECK(launch_plain_dp4a(x, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
+                                   in->s_comp, in->d_err, in->tune.stall, f0, fcount));
+    }
+  } else {
+    const CUtensorMap *map = tensor_map(in, x);
+    if (!map) {
+      fprintf(stderr, "xgpu: cannot describe the input buffer to the tensor memory accelerator\n");
+      return XGPU_CUDA_ERROR;
+    }
+    for (int t0 = 0; t0 < s.t; t0 += kSegment) {
+      const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
+      const int store = ow && t0 == 0;
+      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
+                                 in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount));
+      *tail = !store;   // the next segment follows an adding launch
+    }
+  }
+  return XGPU_OK;
+}
+
 // Queue the engine over one call's device input (any format) on s_comp.
 // input_ready, when given, is the event after which the input is complete
 // (the host-to-device copy); converted formats wait for it on s_conv.
@@ -268,31 +320,9 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   } else if (input_ready) {
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, input_ready, 0));
   }
-  const int ow = in->state_zero ? 1 : 0;
-  if (!in->int_state) {
-    XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
-                                 in->tune.stall));
-  } else if (in->cfg.engine == XGPU_ENGINE_PLAIN) {
-    for (int t0 = 0; t0 < s.t; t0 += kSegment) {
-      const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      XGPU_CHECK(launch_plain_dp4a(x, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
-                                   in->s_comp, in->d_err, in->tune.stall));
-    }
-  } else {
-    const CUtensorMap *map = tensor_map(in, x);
-    if (!map) {
-      fprintf(stderr, "xgpu: cannot describe the input buffer to the tensor memory accelerator\n");
-      return XGPU_CUDA_ERROR;
-    }
-    for (int t0 = 0; t0 < s.t; t0 += kSegment) {
-      const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      const int store = ow && t0 == 0;
-      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
-                                 in->s_comp, in->tune, tail && !store ? 1 : 0));
-      tail = !store;   // the next segment follows an adding launch
-    }
-    in->adding_tail = tail && conv < 0;
-  }
+  const int r = launch_engine(in, x, 0, s.f, &tail);
+  if (r != XGPU_OK) return r;
+  if (in->int_state && in->cfg.engine == XGPU_ENGINE_TENSOR) in->adding_tail = tail && conv < 0;
   in->state_zero = false;
   if (conv >= 0) {
     XGPU_CHECK(cudaEventRecord(in->conv_free[conv], in->s_comp));
@@ -317,6 +347,22 @@ int check_device_error(Internal *in) {
   return XGPU_OK;
 }
 
+// The device address of the caller's output (the host buffer at
+// output_offset) when the formatting kernel can store the dump straight into
+// it: triangular and real-imag orders, whose words the kernel writes in runs,
+// into page-locked memory the device maps, 8-byte aligned.  Those stores
+// cross the host link at the rate of a copy.  Otherwise nullptr: the dump is
+// formatted in device memory and copied.
+void *direct_output(XGPUContext *ctx, Internal *in) {
+  if (in->cfg.matrix_order == REGISTER_TILE_TRIANGULAR_ORDER) return nullptr;
+  void *p = nullptr;
+  if (cudaHostGetDevicePointer(&p, ctx->matrix_h + ctx->output_offset, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return ((uintptr_t)p & 7) == 0 ? p : nullptr;
+}
+
 int dump(XGPUContext *ctx, Internal *in) {
   in->adding_tail = false;
   if (!in->matrix_h_set || !ctx->matrix_h) return XGPU_HOST_BUFFER_NOT_SET;
@@ -326,12 +372,102 @@ int dump(XGPUContext *ctx, Internal *in) {
     XGPU_CHECK(cudaMemsetAsync(in->d_state, 0, (size_t)in->sz.state_elems * (in->int_state ? 8 : 4),
                                in->s_comp));
   }
+  void *direct = direct_output(ctx, in);
   XGPU_CHECK(launch_format(in->d_state, in->int_state ? 0 : 1, in->sz, in->cfg.matrix_order,
-                           in->cfg.output_type, in->d_out, in->s_comp));
-  XGPU_CHECK(cudaMemcpyAsync(ctx->matrix_h + ctx->output_offset, in->d_out,
-                             (size_t)in->sz.mat_length * sizeof(Complex), cudaMemcpyDeviceToHost,
-                             in->s_comp));
+                           in->cfg.output_type, direct ? direct : in->d_out, in->s_comp));
+  if (!direct)
+    XGPU_CHECK(cudaMemcpyAsync(ctx->matrix_h + ctx->output_offset, in->d_out,
+                               (size_t)in->sz.mat_length * sizeof(Complex),
+                               cudaMemcpyDeviceToHost, in->s_comp));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  return check_device_error(in);
+}
+
+// Channel groups for a dumping call over host buffers, 0 when the call goes
+// whole: int8 input only (a converted format is converted in one pass), at
+// least two groups of kGroupMinBytes, an output buffer that takes the dump.
+int dump_groups(XGPUContext *ctx, Internal *in) {
+  const Sizes &s = in->sz;
+  if (in->cfg.input_format != XGPU_INPUT_INT8 || s.f < 2) return 0;
+  if (!in->matrix_h_set || !ctx->matrix_h) return 0;
+  if (ctx->matrix_len && ctx->output_offset + (size_t)s.mat_length > ctx->matrix_len) return 0;
+  long long g = s.input_bytes / kGroupMinBytes;
+  if (g > kMaxGroups) g = kMaxGroups;
+  if (g > s.f) g = s.f;
+  if (g < 2) return 0;
+  const int per = (int)((s.f + g - 1) / g);
+  return (s.f + per - 1) / per;
+}
+
+// xgpuCudaXengine(SYNCOP_DUMP) over host buffers, channel group by channel
+// group, on three streams: each group's channels go host-to-device on s_copy
+// (one 2-D copy: ntime rows of the group's stations), through the engine on
+// s_comp, and through the formatting, which stores either straight into the
+// caller's output on s_dump (direct_output; the engine of group k+1 then runs
+// beside the formatting of group k, on other channels of the buffer) or into
+// device memory on s_comp, copied device-to-host on s_dump.  The input of
+// later groups crosses the host link while the results of earlier ones cross
+// it the other way.  The input copies are all queued before the first
+// device-to-host copy, which may block the host when the output buffer is
+// pageable.  Results are the same as the whole call's: each channel's sums
+// see the same samples in the same order.
+int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
+  const Sizes &s = in->sz;
+  const int per = (s.f + groups - 1) / groups;
+  const size_t row = (size_t)s.n * kNpol * 2;   // bytes of one channel at one sample
+  const size_t pitch = row * s.f;
+  const char *src = (const char *)(ctx->array_h + ctx->input_offset);
+  int8_t *dst = (int8_t *)in->d_in[b];
+  in->adding_tail = false;
+  // The buffer is free once the engine launch that last read it has finished.
+  XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
+  for (int k = 0; k < groups; ++k) {
+    const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
+    XGPU_CHECK(cudaMemcpy2DAsync(dst + f0 * row, pitch, src + f0 * row, pitch, fc * row,
+                                 (size_t)s.t, cudaMemcpyHostToDevice, in->s_copy));
+    XGPU_CHECK(cudaEventRecord(in->group_in[k], in->s_copy));
+  }
+  XGPU_CHECK(cudaEventRecord(in->copy_done[b], in->s_copy));
+  // Direct stores format on s_dump, beside the next group's engine; results
+  // formatted in device memory (register-tile order) format on s_comp and
+  // leave s_dump to the copies.
+  void *direct = direct_output(ctx, in);
+  cudaStream_t s_fmt = direct ? in->s_dump : in->s_comp;
+  for (int k = 0; k < groups; ++k) {
+    const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
+    XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->group_in[k], 0));
+    bool tail = false;
+    int r = launch_engine(in, dst, f0, fc, &tail);
+    if (r != XGPU_OK) return r;
+    if (direct) {
+      XGPU_CHECK(cudaEventRecord(in->group_out[k], in->s_comp));
+      XGPU_CHECK(cudaStreamWaitEvent(in->s_dump, in->group_out[k], 0));
+    }
+    XGPU_CHECK(launch_format(in->d_state, in->int_state ? 0 : 1, s, in->cfg.matrix_order,
+                             in->cfg.output_type, direct ? direct : in->d_out, s_fmt, f0, fc));
+    if (!direct) XGPU_CHECK(cudaEventRecord(in->group_out[k], in->s_comp));
+  }
+  in->state_zero = false;
+  XGPU_CHECK(cudaEventRecord(in->comp_done[b], in->s_comp));
+  if (!direct) {
+    // 32-bit words of the output per channel, and the plane stride (the
+    // real-imag and register-tile orders keep real and imaginary planes).
+    const bool planes = in->cfg.matrix_order != TRIANGULAR_ORDER;
+    const size_t words =
+        planes ? (size_t)(s.mat_length / s.f) : (size_t)(2 * s.mat_length / s.f);
+    char *host = (char *)(ctx->matrix_h + ctx->output_offset);
+    const char *dev = (const char *)in->d_out;
+    for (int k = 0; k < groups; ++k) {
+      const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
+      XGPU_CHECK(cudaStreamWaitEvent(in->s_dump, in->group_out[k], 0));
+      for (int plane = 0; plane < (planes ? 2 : 1); ++plane) {
+        const size_t off = ((size_t)plane * s.mat_length + (size_t)f0 * words) * 4;
+        XGPU_CHECK(cudaMemcpyAsync(host + off, dev + off, (size_t)fc * words * 4,
+                                   cudaMemcpyDeviceToHost, in->s_dump));
+      }
+    }
+  }
+  XGPU_CHECK(cudaStreamSynchronize(in->s_dump));
   return check_device_error(in);
 }
 
@@ -475,8 +611,14 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
       return fail(XGPU_CUDA_ERROR);
   }
   if (cudaStreamCreateWithFlags(&in->s_conv, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&in->s_dump, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&in->caller_ev, cudaEventDisableTiming) != cudaSuccess)
     return fail(XGPU_CUDA_ERROR);
+  for (int k = 0; k < kMaxGroups; ++k) {
+    if (cudaEventCreateWithFlags(&in->group_in[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&in->group_out[k], cudaEventDisableTiming) != cudaSuccess)
+      return fail(XGPU_CUDA_ERROR);
+  }
   if (cudaMemsetAsync(in->d_err, 0, sizeof(int), in->s_comp) != cudaSuccess ||
       cudaMemsetAsync(in->d_state, 0, state_bytes, in->s_comp) != cudaSuccess ||
       cudaStreamSynchronize(in->s_comp) != cudaSuccess)
@@ -614,6 +756,10 @@ int xgpuCudaXengine(XGPUContext *context, int syncOp) {
 
   const int b = in->cur;
   in->cur ^= 1;
+  if (syncOp == SYNCOP_DUMP) {
+    const int groups = dump_groups(context, in);
+    if (groups > 0) return dump_call_grouped(context, in, b, groups);
+  }
   // The buffer is free once the engine launch that last read it has finished.
   XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
   XGPU_CHECK(cudaMemcpyAsync(in->d_in[b], context->array_h + context->input_offset,

@@ -16,7 +16,8 @@ struct Job {
   CUtensorMap map;        // 3-D map {4n bytes, f, t} over the job's int8 input (64-byte aligned)
   int64_t *state;         // triangular int64 integration buffer of the job
   long long nbaseline;    // n(n+1)/2
-  int n, f;
+  int n, f;               // stations; channels of the job's channel range
+  int f0;                 // first channel of the range (channel index into the input and buffer)
   int t0;                 // first sample of the range
   int total_steps;        // pipeline stages (of kTcSamplesPerStage samples) in the range
   int steps_per_split;    // stages per time split
