@@ -506,6 +506,12 @@ def main():
         detail["plain_dp4a_n256_tops"] = ops(N, F, T) / (ms_p * 1e-3) / 1e12
         detail["plain_fp32_n256_tops"] = ops(N, F, T) / (ms_f * 1e-3) / 1e12
         detail["tc_over_plain_dp4a_n256"] = value / world / detail["plain_dp4a_n256_tops"]
+        # the plain engines' own rooflines: measured CUDA-core dp4a and FP32
+        # FMA rates (X-engine operations per second)
+        for kind in ("dp4a", "fp32"):
+            pk = xg.core_peak(kind, local) / 1e12
+            detail[f"core_{kind}_peak_tops_measured"] = pk
+            detail[f"plain_{kind}_n256_frac_of_core_peak"] = detail[f"plain_{kind}_n256_tops"] / pk
         if rank == 0:
             # config 2 itself (every sum below 2^24: exact) and a long
             # integration whose sums pass 2^24

@@ -262,6 +262,13 @@ int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_o
 int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long long seed,
                        double sigma, int device);
 
+/* Measure the device's CUDA-core rate for the plain engines' arithmetic (the
+ * denominator of their rooflines) with a register-resident microbenchmark of
+ * about 25 ms: kind 0 = dp4a, counted as 8 operations (four int8 products and
+ * their sum), kind 1 = FP32 FMA, counted as 2.  *ops_per_second receives the
+ * rate, in the X-engine's operations. */
+int xgpuMeasureCorePeak(int device, int kind, double *ops_per_second);
+
 /* Run the context's device work (engine launches, dump formatting) on the
  * caller's CUDA stream (a cudaStream_t) instead of the context's own, e.g. to
  * order it with other work or to bracket it with the caller's CUDA events.

@@ -141,6 +141,15 @@ def test_errors_before_init(xg):
     L.xgpuFree(p)  # idempotent, as cuda_xengine.cu:537
 
 
+def test_core_peak_arguments_checked_before_any_device_call(xg):
+    L = xg.lib()
+    v = ctypes.c_double(-1.0)
+    assert L.xgpuMeasureCorePeak(0, 2, ctypes.byref(v)) == xg.XGPU_INVALID_ARGUMENT
+    assert L.xgpuMeasureCorePeak(0, -1, ctypes.byref(v)) == xg.XGPU_INVALID_ARGUMENT
+    assert L.xgpuMeasureCorePeak(0, 0, None) == xg.XGPU_INVALID_ARGUMENT
+    assert v.value == -1.0
+
+
 @pytest.mark.parametrize("field,value", [
     ("nstation", 24), ("nstation", 0), ("nfrequency", 0), ("ntimepipe", 8),
     ("ntime", 100), ("compute_type", 7), ("output_type", 0), ("matrix_order", 1234),

@@ -223,6 +223,15 @@ def test_block32_input(xg, oracle_mod, engine, compute):
             assert np.array_equal(got, oracle_mod.xengine_f32(x, n, f, t))
 
 
+def test_core_peaks(xg):
+    """The measured CUDA-core rates are positive, repeatable within 10%, and
+    in the range 148 SMs allow (dp4a: 8 operations each; FMA: 2)."""
+    for kind, lo, hi in (("dp4a", 30e12, 1.2e15), ("fp32", 20e12, 3e14)):
+        a, b = xg.core_peak(kind), xg.core_peak(kind)
+        assert lo < a < hi and lo < b < hi, (kind, a, b)
+        assert abs(a - b) < 0.1 * max(a, b), (kind, a, b)
+
+
 def test_device_generator_matches_host(xg, oracle_mod):
     import torch
     for kind, sigma in [(0, 16.0), (0, 40.0), (1, 0.0), (2, 0.0)]:

@@ -147,6 +147,8 @@ _PROTOTYPES = [
                                                             ctypes.c_void_p]),
     ("xgpuGenerateDevice", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
                                           ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int]),
+    ("xgpuMeasureCorePeak", ctypes.c_int, [ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)]),
     ("xgpuSetComputeStream", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.c_void_p]),
     ("xgpuComputeStream", ctypes.c_void_p, [ctypes.POINTER(XGPUContext)]),
     ("xgpuTuning", ctypes.c_int, [ctypes.POINTER(XGPUContext), ctypes.POINTER(ctypes.c_int),
@@ -445,6 +447,15 @@ def generate_device(ptr, nbytes, kind, seed, sigma=16.0, device=0):
     """Fill device memory with the seeded generator (same bytes as the host one)."""
     return check("xgpuGenerateDevice",
                  lib().xgpuGenerateDevice(ctypes.c_void_p(ptr), nbytes, kind, seed, sigma, device))
+
+
+def core_peak(kind, device=0):
+    """Measured CUDA-core rate in X-engine operations per second: kind
+    "dp4a" (8 per dp4a) or "fp32" (2 per FMA)."""
+    v = ctypes.c_double()
+    check("xgpuMeasureCorePeak",
+          lib().xgpuMeasureCorePeak(device, {"dp4a": 0, "fp32": 1}[kind], ctypes.byref(v)))
+    return v.value
 
 
 def ops_per_integration(n, f, t):
