@@ -331,12 +331,14 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   return XGPU_OK;
 }
 
-// Read and clear the device error word; s_comp must be idle.
-int check_device_error(Internal *in) {
+// Read and clear the device error word.
+// Queued on `st` (default s_comp), which must be the stream whose completion
+// implies every engine launch's: the read and the wait are one round trip.
+int check_device_error(Internal *in, cudaStream_t st = nullptr) {
   in->adding_tail = false;
-  XGPU_CHECK(cudaMemcpyAsync(in->h_err, in->d_err, sizeof(int), cudaMemcpyDeviceToHost,
-                             in->s_comp));
-  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  if (!st) st = in->s_comp;
+  XGPU_CHECK(cudaMemcpyAsync(in->h_err, in->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  XGPU_CHECK(cudaStreamSynchronize(st));
   if (*in->h_err != 0) {
     fprintf(stderr, "xgpu: device wait timed out (code %d); results of this integration are invalid\n",
             *in->h_err);
@@ -379,8 +381,7 @@ int dump(XGPUContext *ctx, Internal *in) {
     XGPU_CHECK(cudaMemcpyAsync(ctx->matrix_h + ctx->output_offset, in->d_out,
                                (size_t)in->sz.mat_length * sizeof(Complex),
                                cudaMemcpyDeviceToHost, in->s_comp));
-  XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
-  return check_device_error(in);
+  return check_device_error(in);   // waits for the formatting and the copy too
 }
 
 // Channel groups for a dumping call over host buffers, 0 when the call goes
@@ -467,8 +468,8 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
       }
     }
   }
-  XGPU_CHECK(cudaStreamSynchronize(in->s_dump));
-  return check_device_error(in);
+  // s_dump's last work follows the last group's engine launch
+  return check_device_error(in, in->s_dump);
 }
 
 int finish_call(XGPUContext *ctx, Internal *in, int syncOp) {
