@@ -540,8 +540,9 @@ def main():
         e2e_v = {"value": ops(N, F, T) / (ms_e * 1e-3) / 1e12, "unit": "TOPS",
                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e,
                  "steps": k_e, "bit_exact_vs_oracle": ok,
-                 # each step copies its input in, then (after the engine and the
-                 # dump formatting) its dump out: the host link sets the pace
+                 # each step copies its input in and its dump out, channel
+                 # group by channel group (the two directions overlap): the
+                 # host link sets the pace
                  "host_link_gbs": (h2d + d2h) / (ms_e * 1e-3) / 1e9}
     clk = clocks.stop()
     peak8 = int8_peak_tops(torch) if rank == 0 else None
