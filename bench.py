@@ -151,13 +151,14 @@ TUNING = {}   # (engine, n, f, t) -> the tensor engine's autotuned setting
 
 
 def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, seed=1,
-                     sigma=SIGMA, min_rotate_bytes=2 * L2_BYTES, max_bufs=16):
+                     sigma=SIGMA, min_rotate_bytes=2 * L2_BYTES, max_bufs=16, tune=None):
     """Average ms per xgpuCudaXengineDevice call (input resident in HBM).  The
-    tensor engine's time splits and grid come from the library's autotuner."""
+    tensor engine's time splits and grid come from the library's autotuner, or
+    from `tune` = (ksplit, grid, pair)."""
     c = xg.Correlator(n, f, t, engine=engine, compute=compute, output="int32", order="tri",
                       device=torch.cuda.current_device())
     if engine == "tensor":
-        c.tune(0)   # kernel, time splits and grid chosen by timing
+        c.tune(*tune) if tune else c.tune(0)   # kernel, time splits and grid chosen by timing
     # The timing events go on the context's own stream, where consecutive
     # accumulating calls may overlap (programmatic dependent launch).
     stream = torch.cuda.ExternalStream(c.stream)
@@ -471,6 +472,9 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--tune", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
+                    help="ksplit,grid,pair for the headline leg instead of the autotuner (a "
+                         "profiler's serialised launches mislead the autotuner)")
     ap.add_argument("--no-detail", action="store_true",
                     help="skip the plain, N=512, batched and served legs")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
@@ -492,7 +496,7 @@ def main():
 
     # headline: tensor engine, config 2, input resident in HBM
     ms, rot_bytes = device_engine_ms(xg, torch, "tensor", "int8", N, F, T, args.steps,
-                                     args.warmup, world)
+                                     args.warmup, world, tune=args.tune)
     ms = max_over_ranks(world, ms)
     value = world * ops(N, F, T) / (ms * 1e-3) / 1e12
 
