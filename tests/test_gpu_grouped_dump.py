@@ -113,3 +113,33 @@ def test_grouped_dump_caller_buffers_and_offsets(xg, oracle_mod, flags):
         assert L.xgpuCudaXengine(ctypes.byref(ctx), xg.SYNCOP_DUMP) == xg.XGPU_INVALID_ARGUMENT
     finally:
         L.xgpuFree(ctypes.byref(ctx))
+
+
+@pytest.mark.parametrize("engine,compute", [("tensor", "int8"), ("plain", "int8")])
+def test_grouped_dump_on_caller_stream(xg, oracle_mod, engine, compute):
+    """With the context's work on the caller's stream (xgpuSetComputeStream),
+    the grouped dump orders its groups' engine launches after earlier work on
+    that stream and returns complete results."""
+    import torch
+    n, f, t = 128, 6, 1024
+    xs = [oracle_mod.gaussian_input(n, f, t, seed=500 + k, sigma=25.0) for k in range(2)]
+    exact = sum(oracle_mod.xengine_i64(x, n, f, t) for x in xs)
+    stream = torch.cuda.Stream()
+    with xg.Correlator(n, f, t, engine=engine, compute=compute) as c:
+        c.set_stream(stream.cuda_stream)
+        c.set_input(xs[0])
+        c.run(xg.SYNCOP_SYNC_TRANSFER)
+        # unrelated work queued on the caller's stream between the calls
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(1000000)
+        c.set_input(xs[1])
+        c.run(xg.SYNCOP_DUMP)
+        out = c.output_view()[: c.info.matLength * 2].copy()
+        assert np.array_equal(out, exact.astype(np.int32))
+        assert np.array_equal(c.dump_int64(), exact)
+        c.set_stream(None)
+        c.clear()
+        c.set_input(xs[0])
+        c.run(xg.SYNCOP_DUMP)
+        out = c.output_view()[: c.info.matLength * 2].copy()
+        assert np.array_equal(out, oracle_mod.xengine_i64(xs[0], n, f, t).astype(np.int32))
