@@ -49,3 +49,22 @@ def test_plain_engine_expired_wait_is_reported_and_recoverable(xg, oracle_mod, c
         got = c.output_view()[: c.info.matLength * 2].copy()
     exact = oracle_mod.xengine_i64(x, n, f, t)
     assert np.array_equal(got, exact.astype(got.dtype))
+
+
+def test_packed_input_pair_kernel_expired_wait_is_reported_and_recoverable(xg, oracle_mod):
+    """Packed input expanded inside the CTA-pair kernel: with the loads
+    withheld, the converter warps' waits expire the same way."""
+    n, f, t = 128, 2, 1024
+    packed = oracle_mod.generate(t * f * n * 2, 1, 77)
+    with xg.Correlator(n, f, t, engine="tensor", input_format="packed4") as c:
+        c.tune(1, 0, 1)
+        c.set_input(packed)
+        assert xg.lib().xgpuInjectTimeout(ctypes.byref(c.ctx), 1) == 0
+        with pytest.raises(xg.XGPUError) as err:
+            c.run(xg.SYNCOP_SYNC_COMPUTE)
+        assert err.value.code == xg.XGPU_CUDA_ERROR
+        assert xg.lib().xgpuInjectTimeout(ctypes.byref(c.ctx), 0) == 0
+        c.clear()
+        c.run(xg.SYNCOP_DUMP)
+        got = c.dump_int64()
+    assert np.array_equal(got, oracle_mod.xengine_i64(oracle_mod.unpack4(packed), n, f, t))

@@ -430,12 +430,33 @@ def test_long_overlapping_integration_past_int32(xg, oracle_mod, pair):
 @pytest.mark.parametrize("n,f,t,tune", [(48, 2, 1040, (1, 0, 0)),    # partial block and stage
                                         (64, 3, 512, (3, 0, 0)),     # time splits
                                         (128, 2, 2048, (1, 0, 2)),   # stream-K shares
-                                        (96, 1, 256, (1, 0, 1)),     # CTA pairs: pre-pass
+                                        (96, 1, 256, (1, 0, 1)),     # CTA pairs: expanded in-kernel
                                         (32, 1, 65536 + 256, (1, 0, 0))])   # three segments
 def test_packed4_tensor_paths(xg, oracle_mod, n, f, t, tune):
-    """Packed 4+4-bit input on the tensor engine, expanded by the pre-pass, with
-    each kernel choice, partial station blocks and stages, and long calls."""
+    """Packed 4+4-bit input on the tensor engine (expanded by the pre-pass for
+    the single-CTA kernel, in shared memory by the CTA-pair kernel), with each
+    kernel choice, partial station blocks and stages, and long calls."""
     packed = oracle_mod.generate(t * f * n * 2, 1, n + t)
+    exact = oracle_mod.xengine_i64(oracle_mod.unpack4(packed), n, f, t)
+    with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor", input_format="packed4") as c:
+        c.tune(*tune)
+        c.set_input(packed)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)     # stores into the cleared buffer
+        c.run(xg.SYNCOP_DUMP)             # adds
+        assert np.array_equal(c.dump_int64(), 2 * exact)
+
+
+@pytest.mark.parametrize("n,f,t,tune", [(96, 1, 256, (1, 0, 1)),      # one diagonal tile, partial block
+                                        (48, 3, 1040, (1, 0, 1)),     # partial stage
+                                        (256, 4, 2048, (3, 0, 1)),    # off-diagonal tiles, time splits
+                                        (512, 2, 1024, (1, 24, 1)),   # several items per CTA pair
+                                        (64, 2, 32768 + 384, (1, 0, 1))])   # two segments
+def test_packed4_expanded_in_pair_kernel(xg, oracle_mod, n, f, t, tune):
+    """Packed input on the CTA-pair kernel is expanded in shared memory, with
+    no pre-pass.  Random bytes cover every packed value (-8..7 in both
+    nibbles); the sums must equal the oracle's, stored and then added."""
+    rng = np.random.default_rng(n * 7 + t)
+    packed = rng.integers(0, 256, t * f * n * 2, dtype=np.uint8).view(np.int8)
     exact = oracle_mod.xengine_i64(oracle_mod.unpack4(packed), n, f, t)
     with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor", input_format="packed4") as c:
         c.tune(*tune)

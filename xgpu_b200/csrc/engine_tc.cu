@@ -455,6 +455,20 @@ int make_panel_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int row
   return input_map(map, dev_in, s, rows, CU_TENSOR_MAP_SWIZZLE_NONE);
 }
 
+int make_packed_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return -1;
+  if (((uintptr_t)dev_in & 15) != 0 || s.n % 8 != 0) return -2;
+  cuuint64_t dims[3] = {(cuuint64_t)2 * s.n, (cuuint64_t)s.f, (cuuint64_t)s.t};
+  cuuint64_t strides[2] = {(cuuint64_t)2 * s.n, (cuuint64_t)2 * s.n * s.f};
+  cuuint32_t box[3] = {(cuuint32_t)tc::kTile / 2, 1, (cuuint32_t)tc::kKt};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(dev_in), dims,
+                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -3;
+}
+
 int current_device_sms() {
   static std::atomic<int> cache[kDeviceCache];
   int dev = 0;
@@ -528,11 +542,13 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune, int overlap, int f0, int fcount) {
+                            const TcTuning &tune, int overlap, int f0, int fcount, int packed) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   if (tune.wide)
-    return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap, f0, fcount);
+    return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap, f0, fcount,
+                      packed);
+  if (packed) return cudaErrorInvalidValue;   // only the CTA-pair kernel expands packed input
   const int sms = current_device_sms();
   if (!sms) return cudaErrorInvalidDevice;
   {

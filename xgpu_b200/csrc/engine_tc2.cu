@@ -58,6 +58,18 @@ constexpr uint32_t kAccCols = 2 * kHalf;    // 256 columns per accumulator
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kThreads = 192;
 constexpr uint32_t kIdesc = i8_idesc(2 * kHalf, 2 * kHalf);
+// Packed 4+4-bit input (one byte per complex sample, 2n bytes per sample):
+// each CTA loads its 32 stations' packed bytes (64 per sample) into the upper
+// half of an operand box, and converter warps expand them in place into the
+// int8 layout the MMA reads.  One converter warp owns each pipeline slot, so
+// every slot's phases are waited on in order.
+constexpr int kPackedRow = kStations * 2;     // 64 packed bytes per sample
+constexpr int kPackedBox = kPackedRow * kKt;  // 8 KiB
+constexpr int kConvWarps = kStages;
+constexpr int kThreadsPacked = kThreads + 32 * kConvWarps;
+// barriers (24 slots), work-item ring, TMEM slot and abort flag, then the
+// packed-input slot barriers and slot contents
+static_assert(24 * 8 + kSched * 64 + 8 + kStages * 9 <= kBarrierBytes, "barrier area");
 
 struct Params {
   Job job;             // the job when jobs == nullptr (npairs counts 256x256 tiles)
@@ -206,13 +218,55 @@ __device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint64_t adesc, uint64
       : "memory");
 }
 
+// Packed input: 4 packed samples (one word, real part in each byte's high
+// nibble, imaginary part in its low nibble) -> 8 int8 bytes {re, im, ...},
+// each 16 times the 4-bit two's-complement value: a nibble moved to (or left
+// in) the high half of its byte is already that multiple, and |16 x 7| = 112
+// fits int8.  The Gram sums then come out exactly 256 times too large, and the
+// drain divides them back (unscale).
+__device__ __forceinline__ uint2 expand_scaled(uint32_t w) {
+  const uint32_t re = w & 0xF0F0F0F0u, im = (w << 4) & 0xF0F0F0F0u;
+  return make_uint2(__byte_perm(re, im, 0x5140), __byte_perm(re, im, 0x7362));
+}
+
+template <bool kPacked>
+__device__ __forceinline__ long long unscale(long long v) {
+  return kPacked ? v >> 8 : v;   // exact: every packed-input sum is a multiple of 256
+}
+
+// Expands, in place, the packed panel that TMA wrote into the upper half of a
+// 16 KiB operand box (128 samples x 64 bytes) into the box itself: 128 samples
+// x 128 int8 bytes in the 128-byte swizzled layout (16-byte chunk j of sample
+// row r at r*128 + ((j ^ (r & 7)) << 4)).  Lane l handles 16 packed bytes of
+// each 8-sample block b (row 8b + l/4, chunks 2(l%4) and 2(l%4)+1).  Every lane
+// reads all its packed bytes before any lane writes, so no packed byte is
+// overwritten before it is read.
+__device__ __forceinline__ void expand_box(uint8_t *box, int lane) {
+  const uint8_t *packed = box + kPackedBox;
+  uint4 w[kKt / 8];
+#pragma unroll
+  for (int b = 0; b < kKt / 8; ++b) w[b] = *(const uint4 *)(packed + b * 512 + lane * 16);
+  __syncwarp();
+  const int j = (lane & 3) * 2;
+#pragma unroll
+  for (int b = 0; b < kKt / 8; ++b) {
+    const int r = b * 8 + (lane >> 2);
+    const uint2 e0 = expand_scaled(w[b].x), e1 = expand_scaled(w[b].y);
+    const uint2 e2 = expand_scaled(w[b].z), e3 = expand_scaled(w[b].w);
+    uint8_t *row = box + r * 128;
+    *(uint4 *)(row + ((j ^ (r & 7)) << 4)) = make_uint4(e0.x, e0.y, e1.x, e1.y);
+    *(uint4 *)(row + (((j + 1) ^ (r & 7)) << 4)) = make_uint4(e2.x, e2.y, e3.x, e3.y);
+  }
+}
+
 __device__ __forceinline__ void commit_pair(uint32_t cluster_bar) {
   asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    cluster_bar)
                : "memory");
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+template <bool kPacked>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPacked : kThreads, 1)
     xengine_tc2_kernel(const __grid_constant__ Params p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -227,6 +281,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   Item *ring = (Item *)(bars + 2 * kStages + 6 + 2 * kSched);
   uint32_t *tmem_slot = (uint32_t *)(ring + kSched);
   volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+  // packed input: the slots' packed-load barriers, and each slot's content
+  // (0: A and B boxes, 1: A only (diagonal tile), -1: no more stages)
+  const uint32_t raw0 = smem_u32(tmem_slot + 2);
+  volatile signed char *stage_info = (volatile signed char *)(tmem_slot + 2 + 2 * kStages);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_rank();
@@ -242,8 +300,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   }
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(full0 + 8 * s, 1);     // the leader's arrival; both CTAs' loads complete on it
+      // int8 input: the leader's arrival, and both CTAs' loads complete on it;
+      // packed input: one converter warp of each CTA
+      mbar_init(full0 + 8 * s, kPacked ? 2 : 1);
       mbar_init(empty0 + 8 * s, 1);
+      if (kPacked) mbar_init(raw0 + 8 * s, 1);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(tfull0 + 8 * a, 1);
@@ -326,13 +387,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           }
           if (p.stall) continue;
           const uint32_t dst = stage0 + s * kStageBytes;
-          const uint32_t fbar = peer_addr(full0 + 8 * s, 0);
-          // The leader expects the bytes of both CTAs; the peer's loads may land
-          // first (the transaction count then dips below zero until it does).
-          if (leader) mbar_expect_tx(full0 + 8 * s, diag ? 2 * kBoxBytes : 4 * kBoxBytes);
           const int z = t.t0 + (t.step0 + ks) * kKt;
-          tma_load_3d_pair(dst, t.map, fbar, rb * kHalf, t.f, z);
-          if (!diag) tma_load_3d_pair(dst + kBoxBytes, t.map, fbar, cbb * kHalf, t.f, z);
+          if (kPacked) {
+            // this CTA's packed rows into the upper halves of its boxes, for
+            // its own converter warp
+            stage_info[s] = diag ? 1 : 0;
+            mbar_expect_tx(raw0 + 8 * s, diag ? kPackedBox : 2 * kPackedBox);
+            tma_load_3d(dst + kPackedBox, t.map, raw0 + 8 * s, rb * kPackedRow, t.f, z);
+            if (!diag)
+              tma_load_3d(dst + kBoxBytes + kPackedBox, t.map, raw0 + 8 * s, cbb * kPackedRow,
+                          t.f, z);
+          } else {
+            const uint32_t fbar = peer_addr(full0 + 8 * s, 0);
+            // The leader expects the bytes of both CTAs; the peer's loads may land
+            // first (the transaction count then dips below zero until it does).
+            if (leader) mbar_expect_tx(full0 + 8 * s, diag ? 2 * kBoxBytes : 4 * kBoxBytes);
+            tma_load_3d_pair(dst, t.map, fbar, rb * kHalf, t.f, z);
+            if (!diag) tma_load_3d_pair(dst + kBoxBytes, t.map, fbar, cbb * kHalf, t.f, z);
+          }
+        }
+      }
+      if (kPacked && !p.stall) {
+        // No stage follows: tell each converter warp, in its slot's next phase.
+        for (int e = 0; e < kConvWarps && !*abort_flag; ++e, ++g) {
+          const uint32_t s = g % kStages;
+          if (g >= (uint32_t)kStages &&
+              !mbar_wait(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort_flag)) {
+            fail(kErrTimeoutProducer);
+            break;
+          }
+          stage_info[s] = -1;
+          mbar_arrive(raw0 + 8 * s);
         }
       }
     }
@@ -361,7 +446,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         const uint32_t d = tmem + (uint32_t)(acc * kAccCols);
         for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
           const uint32_t s = g % kStages;
-          if (!mbar_wait(full0 + 8 * s, (g / kStages) & 1, abort_flag)) {
+          // packed input: both CTAs' converters arrived (the peer's from its CTA)
+          if (!(kPacked ? mbar_wait_cluster(full0 + 8 * s, (g / kStages) & 1, abort_flag)
+                        : mbar_wait(full0 + 8 * s, (g / kStages) & 1, abort_flag))) {
             fail(kErrTimeoutMma);
             ok = false;
             break;
@@ -388,7 +475,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         mbar_wait(mma_done, 0, nullptr);
       }
     }
-  } else {
+  } else if (!kPacked || warp < 6) {
     // ---------------------------------------------------------- epilogue --
     // Two schedules.  Joint: the four warps drain a column block, meet at a
     // barrier, and warp 0 hands all 32 staging rows to the bulk-copy engine.
@@ -454,8 +541,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
               const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
               const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
               const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
-              const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
-              const long long im = c ? (long long)v2 - rb2 : (long long)ra - v1;
+              const long long re = unscale<kPacked>(c ? (long long)ra + v3 : (long long)v0 + rb2);
+              const long long im = unscale<kPacked>(c ? (long long)v2 - rb2 : (long long)ra - v1);
               const int jl = q * 8 + jj;
               if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
             }
@@ -539,8 +626,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
               const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
               const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
               const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
-              const long long re = c ? (long long)ra + v3 : (long long)v0 + rb2;
-              const long long im = c ? (long long)v2 - rb2 : (long long)ra - v1;
+              const long long re = unscale<kPacked>(c ? (long long)ra + v3 : (long long)v0 + rb2);
+              const long long im = unscale<kPacked>(c ? (long long)v2 - rb2 : (long long)ra - v1);
               const int jl = q * 8 + jj;
               if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
             }
@@ -566,6 +653,32 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       }
       if (copier) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
+  } else {
+    // -------------------------------------------------------- converters --
+    // Packed input only.  Converter warp w owns pipeline slot w: for each of
+    // the slot's stages it waits for this CTA's packed loads, expands the A
+    // box (and the B box off the diagonal) in place, makes the bytes visible
+    // to the tensor cores and reports the stage on the leader's barrier.
+    const int w = warp - 6;
+    const uint32_t fullw = leader ? full0 + 8 * w : peer_addr(full0 + 8 * w, 0);
+    for (uint32_t k = 0;; ++k) {
+      const bool got = mbar_wait(raw0 + 8 * w, k & 1, abort_flag);
+      if (!__all_sync(0xffffffffu, got)) {
+        if (lane == 0) fail(kErrTimeoutConvert);
+        break;
+      }
+      const int info = stage_info[w];
+      if (info < 0) break;
+      uint8_t *box = smem + w * kStageBytes;
+      expand_box(box, lane);
+      if (info == 0) expand_box(box + kBoxBytes, lane);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        if (leader) mbar_arrive(fullw);
+        else remote_arrive(fullw);
+      }
+    }
   }
 
   __syncwarp();   // lanes 1-31 of the producer and MMA warps wait for lane 0
@@ -584,13 +697,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 }  // namespace tc2
 
 cudaError_t tc2_set_smem_attribute() {
-  return cudaFuncSetAttribute(tc2::xengine_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              tc2::kSmemBytes);
+  cudaError_t e = cudaFuncSetAttribute(tc2::xengine_tc2_kernel<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, tc2::kSmemBytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(tc2::xengine_tc2_kernel<true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, tc2::kSmemBytes);
 }
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap,
-                       int f0, int fcount) {
+                       int f0, int fcount, int packed) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   const int num_sms = current_device_sms();
@@ -643,7 +759,7 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   // tail (the kernel waits for it before touching global memory).
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(2 * clusters));
-  cfg.blockDim = dim3(tc2::kThreads);
+  cfg.blockDim = dim3(packed ? tc2::kThreadsPacked : tc2::kThreads);
   cfg.dynamicSmemBytes = tc2::kSmemBytes;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -651,7 +767,8 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, tc2::xengine_tc2_kernel, p);
+  return packed ? cudaLaunchKernelEx(&cfg, tc2::xengine_tc2_kernel<true>, p)
+                : cudaLaunchKernelEx(&cfg, tc2::xengine_tc2_kernel<false>, p);
 }
 
 cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -677,7 +794,7 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
   int clusters = (grid > 0 ? grid : sms) / 2;
   if (clusters > total_items) clusters = total_items;
   if (clusters < 1) return cudaSuccess;
-  tc2::xengine_tc2_kernel<<<2 * clusters, tc2::kThreads, tc2::kSmemBytes, st>>>(p);
+  tc2::xengine_tc2_kernel<false><<<2 * clusters, tc2::kThreads, tc2::kSmemBytes, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -26,6 +26,7 @@ enum DeviceError : int {
   kErrTimeoutMma = 2,        // MMA issuer gave up waiting for a loaded stage
   kErrTimeoutDrain = 3,      // epilogue gave up waiting for the accumulator
   kErrTimeoutPanel = 4,      // plain engine gave up waiting for an input panel
+  kErrTimeoutConvert = 5,    // packed-input converter gave up waiting for a loaded stage
 };
 
 struct Sizes {
@@ -70,13 +71,16 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 // commuting.  Channels [f0, f0 + fcount) of the input and buffer are
 // correlated (fcount < 0: through the last channel); an overwrite stores into,
 // or clears, that channel range only.
+// packed = 1: `map` describes packed 4+4-bit input (make_packed_map), which
+// the CTA-pair kernel expands in shared memory; it needs tune.wide.
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune, int overlap, int f0 = 0, int fcount = -1);
+                            const TcTuning &tune, int overlap, int f0 = 0, int fcount = -1,
+                            int packed = 0);
 // The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune,
-                       int overlap, int f0 = 0, int fcount = -1);
+                       int overlap, int f0 = 0, int fcount = -1, int packed = 0);
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -97,6 +101,10 @@ int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);
 // The same map with unswizzled boxes of 128 bytes x `rows` samples (the plain
 // engines' panels).
 int make_panel_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int rows);
+// {x: 2n bytes, y: f, z: t} over packed 4+4-bit input [t][f][s][p], unswizzled
+// boxes of 64 bytes (32 stations) x 128 samples: the CTA-pair kernel's packed
+// loads.  Needs n a multiple of 8.  Returns 0 on success.
+int make_packed_map(CUtensorMap *map, const void *dev_in, const Sizes &s);
 // 0 if the tensor-core kernel image loads on the current device.
 cudaError_t tc_check_device();
 // Per-device set-up and facts, cached for devices 0 .. kDeviceCache-1 (others are

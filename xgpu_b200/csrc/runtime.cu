@@ -106,6 +106,7 @@ struct Internal {
   // tensor maps, cached by device pointer
   struct MapEntry {
     const void *ptr;
+    bool packed;     // packed 4+4-bit geometry (make_packed_map)
     CUtensorMap map;
   } maps[4];
   int nmaps = 0;
@@ -239,23 +240,36 @@ cudaError_t register_range(void *p, size_t bytes, void **registered) {
   return e;
 }
 
-const CUtensorMap *tensor_map(Internal *in, const void *ptr) {
+const CUtensorMap *tensor_map(Internal *in, const void *ptr, bool packed = false) {
   for (int q = 0; q < in->nmaps; ++q)
-    if (in->maps[q].ptr == ptr) return &in->maps[q].map;
+    if (in->maps[q].ptr == ptr && in->maps[q].packed == packed) return &in->maps[q].map;
   const int slot = in->nmaps < 4 ? in->nmaps++ : 3;
-  if (make_tc_tensor_map(&in->maps[slot].map, ptr, in->sz) != 0) {
+  const int r = packed ? make_packed_map(&in->maps[slot].map, ptr, in->sz)
+                       : make_tc_tensor_map(&in->maps[slot].map, ptr, in->sz);
+  if (r != 0) {
     in->maps[slot].ptr = nullptr;
     return nullptr;
   }
   in->maps[slot].ptr = ptr;
+  in->maps[slot].packed = packed;
   return &in->maps[slot].map;
 }
 
-// Queue the engine over channels [f0, f0 + fcount) of int8 input x on s_comp,
-// in time segments; the first segment stores when the buffer is known to be
-// zero.  *tail: in, the launch may overlap the adding launch before it; out,
-// the last launch queued only added.
-int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail) {
+// Packed 4+4-bit input goes straight to the CTA-pair kernel, which expands it
+// in shared memory; other kernels (and engines) read it converted to int8 by a
+// pre-pass.
+bool packed_in_kernel(const Internal *in) {
+  return in->cfg.input_format == XGPU_INPUT_PACKED4 && in->int_state &&
+         in->cfg.engine == XGPU_ENGINE_TENSOR && in->tune.wide;
+}
+
+// Queue the engine over channels [f0, f0 + fcount) of int8 input x (packed
+// input when `packed`: packed_in_kernel) on s_comp, in time segments; the
+// first segment stores when the buffer is known to be zero.  *tail: in, the
+// launch may overlap the adding launch before it; out, the last launch queued
+// only added.
+int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail,
+                  bool packed = false) {
   const Sizes &s = in->sz;
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
@@ -268,7 +282,7 @@ int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail)
                                    in->s_comp, in->d_err, in->tune.stall, f0, fcount));
     }
   } else {
-    const CUtensorMap *map = tensor_map(in, x);
+    const CUtensorMap *map = tensor_map(in, x, packed);
     if (!map) {
       fprintf(stderr, "xgpu: cannot describe the input buffer to the tensor memory accelerator\n");
       return XGPU_CUDA_ERROR;
@@ -277,7 +291,8 @@ int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail)
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
       const int store = ow && t0 == 0;
       XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
-                                 in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount));
+                                 in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount,
+                                 packed ? 1 : 0));
       *tail = !store;   // the next segment follows an adding launch
     }
   }
@@ -297,7 +312,8 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   bool tail = in->adding_tail && in->s_comp == in->s_own && !input_ready &&
               in->cfg.input_format == XGPU_INPUT_INT8;
   in->adding_tail = false;
-  if (in->cfg.input_format != XGPU_INPUT_INT8) {
+  const bool packed = packed_in_kernel(in);
+  if (in->cfg.input_format != XGPU_INPUT_INT8 && !packed) {
     conv = in->conv_cur;
     in->conv_cur ^= 1;
     if (in->conv_used[conv]) XGPU_CHECK(cudaStreamWaitEvent(in->s_conv, in->conv_free[conv], 0));
@@ -320,7 +336,7 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   } else if (input_ready) {
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, input_ready, 0));
   }
-  const int r = launch_engine(in, x, 0, s.f, &tail);
+  const int r = launch_engine(in, x, 0, s.f, &tail, packed);
   if (r != XGPU_OK) return r;
   if (in->int_state && in->cfg.engine == XGPU_ENGINE_TENSOR) in->adding_tail = tail && conv < 0;
   in->state_zero = false;
