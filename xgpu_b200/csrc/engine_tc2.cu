@@ -237,25 +237,24 @@ __device__ __forceinline__ long long unscale(long long v) {
 // Expands, in place, the packed panel that TMA wrote into the upper half of a
 // 16 KiB operand box (128 samples x 64 bytes) into the box itself: 128 samples
 // x 128 int8 bytes in the 128-byte swizzled layout (16-byte chunk j of sample
-// row r at r*128 + ((j ^ (r & 7)) << 4)).  Lane l handles 16 packed bytes of
-// each 8-sample block b (row 8b + l/4, chunks 2(l%4) and 2(l%4)+1).  Every lane
-// reads all its packed bytes before any lane writes, so no packed byte is
-// overwritten before it is read.
+// row r at r*128 + ((j ^ (r & 7)) << 4)).  In pass q, lane l makes chunk
+// j = l%8 of row r = 4q + l/8 from the row's packed bytes 8j .. 8j+7, so each
+// group of eight lanes reads 64 consecutive bytes and writes the eight chunks
+// of one row (all 32 banks once).  Every lane reads all its packed bytes
+// before any lane writes, so no packed byte is overwritten before it is read.
 __device__ __forceinline__ void expand_box(uint8_t *box, int lane) {
   const uint8_t *packed = box + kPackedBox;
-  uint4 w[kKt / 8];
+  const int j = lane & 7;
+  uint2 w[kKt / 4];
 #pragma unroll
-  for (int b = 0; b < kKt / 8; ++b) w[b] = *(const uint4 *)(packed + b * 512 + lane * 16);
+  for (int q = 0; q < kKt / 4; ++q)
+    w[q] = *(const uint2 *)(packed + (4 * q + (lane >> 3)) * kPackedRow + j * 8);
   __syncwarp();
-  const int j = (lane & 3) * 2;
 #pragma unroll
-  for (int b = 0; b < kKt / 8; ++b) {
-    const int r = b * 8 + (lane >> 2);
-    const uint2 e0 = expand_scaled(w[b].x), e1 = expand_scaled(w[b].y);
-    const uint2 e2 = expand_scaled(w[b].z), e3 = expand_scaled(w[b].w);
-    uint8_t *row = box + r * 128;
-    *(uint4 *)(row + ((j ^ (r & 7)) << 4)) = make_uint4(e0.x, e0.y, e1.x, e1.y);
-    *(uint4 *)(row + (((j + 1) ^ (r & 7)) << 4)) = make_uint4(e2.x, e2.y, e3.x, e3.y);
+  for (int q = 0; q < kKt / 4; ++q) {
+    const int r = 4 * q + (lane >> 3);
+    const uint2 e0 = expand_scaled(w[q].x), e1 = expand_scaled(w[q].y);
+    *(uint4 *)(box + r * 128 + ((j ^ (r & 7)) << 4)) = make_uint4(e0.x, e0.y, e1.x, e1.y);
   }
 }
 
