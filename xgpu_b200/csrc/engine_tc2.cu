@@ -24,6 +24,11 @@
 // Like engine_tc.cu the kernel is launched programmatically (an adding launch
 // may run beside the previous one), and its epilogue has two schedules, joint
 // and split per warp, chosen by the length of the launch's items.
+// A second instantiation (kPacked) reads packed 4+4-bit input: each CTA's
+// producer loads the packed bytes into the upper halves of its operand boxes,
+// five converter warps (one per pipeline slot) expand them in place, scaled by
+// 16, and report each stage on the leader's "full" barrier; the drain divides
+// the sums by 256.
 #include <cudaTypedefs.h>
 #include <string.h>
 
