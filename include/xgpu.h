@@ -313,7 +313,9 @@ int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGP
  * exactly in the integration buffer; grid is the number of CTAs (0 = one per
  * SM).  ksplit = 0 autotunes all three now: the engine is timed on synthetic
  * input and a scratch integration buffer (the context's own is not touched)
- * and the fastest setting is kept. */
+ * and the fastest setting is kept.  With CTA pairs, XGPU_INPUT_PACKED4 input
+ * is expanded inside the kernel; the other kernels read an int8 copy that a
+ * pre-pass makes. */
 int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);
 
 /* The setting in use (as xgpuTune takes it; ksplit >= 1), e.g. to keep an
