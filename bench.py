@@ -408,6 +408,18 @@ def int8_peak_tops(torch):
         return None
 
 
+def cpu_model():
+    """The host CPU's model name (for the CPU baseline's record), or None."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(steps_cap=None, budget_s=12.0):
     """The reference's xgpuOmpXengine on the host, DP4A build, this workload."""
     import oracle
@@ -428,7 +440,7 @@ def cpu_baseline(steps_cap=None, budget_s=12.0):
             break
     med = statistics.median(times)
     return {"value": ops(N, F, T) / med / 1e12, "unit": "TOPS", "cores": os.cpu_count(),
-            "kind": "reference",
+            "kind": "reference", "cpu_model": cpu_model(),
             "sample": f"{len(times)} full calls of xgpuOmpXengine (src/omp_xengine.c, -O3 -fopenmp, "
                       f"DP4A build) at N={N} F={F} T={T}; median {med * 1e3:.1f} ms per call",
             "ms_per_call": med * 1e3}
@@ -459,6 +471,7 @@ def run_reference(args, world, rank):
         "config": {"workload": f"xgpuOmpXengine NSTATION={N} NPOL=2 NFREQUENCY={F} NTIME={T}, "
                                "one call per step", "nstation": N, "nfrequency": F, "ntime": T},
         "cpu_baseline": {"value": v, "unit": "TOPS", "cores": os.cpu_count(), "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": f"{args.steps} calls of the reference xgpuOmpXengine (DP4A "
                                    "build, OpenMP on all host cores)"},
         "e2e": {"value": v, "unit": "TOPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
