@@ -68,7 +68,8 @@ struct Internal {
   bool int_state = true;  // int64 buffer (integer engines) or float (FP32)
 
   void *d_in[2] = {nullptr, nullptr};  // one call's input, as supplied
-  // Packed 4+4-bit, DP4A-swizzled and block-32 input is converted to int8
+  // Packed 4+4-bit (unless the CTA-pair kernel expands it itself:
+  // packed_in_kernel), DP4A-swizzled and block-32 input is converted to int8
   // [t][f][s][p][c] on its own stream into one of two buffers, so the
   // conversion of call k+1 is queued without waiting for the engine of call
   // k (measured: the two kernels seldom share the SMs, so a converted call
