@@ -143,3 +143,21 @@ def test_grouped_dump_on_caller_stream(xg, oracle_mod, engine, compute):
         c.run(xg.SYNCOP_DUMP)
         out = c.output_view()[: c.info.matLength * 2].copy()
         assert np.array_equal(out, oracle_mod.xengine_i64(xs[0], n, f, t).astype(np.int32))
+
+
+def test_grouped_dump_packed_input_on_cta_pairs(xg, oracle_mod):
+    """Packed 4+4-bit input that the CTA-pair kernel expands also goes in
+    channel groups (one packed byte per station and polarisation per row of
+    the 2-D copies); every byte value, stored and then added."""
+    n, f, t = 256, 16, 1024                 # 8.4 MB packed: 8 groups of 2 channels
+    rng = np.random.default_rng(2024)
+    packed = rng.integers(0, 256, t * f * n * 2, dtype=np.uint8).view(np.int8)
+    exact = oracle_mod.xengine_i64(oracle_mod.unpack4(packed), n, f, t)
+    with xg.Correlator(n, f, t, engine="tensor", input_format="packed4") as c:
+        c.tune(1, 0, 1)
+        c.set_input(packed)
+        c.run(xg.SYNCOP_DUMP)
+        out = c.output_view()[: c.info.matLength * 2].copy()
+        assert np.array_equal(out, exact.astype(np.int32))
+        c.run(xg.SYNCOP_DUMP)
+        assert np.array_equal(c.dump_int64(), 2 * exact)

@@ -466,6 +466,27 @@ def test_packed4_expanded_in_pair_kernel(xg, oracle_mod, n, f, t, tune):
         assert np.array_equal(c.dump_int64(), 2 * exact)
 
 
+def test_packed4_overlapping_calls_on_cta_pairs(xg, oracle_mod):
+    """Accumulating device calls of packed input on CTA pairs (expanded in the
+    kernel, no conversion between them) overlap on the context's stream and
+    stay exact, across a clear and with several 32768-sample segments."""
+    import torch
+    n, f, t = 128, 3, 65536 + 256
+    ps = [oracle_mod.generate(t * f * n * 2, 1, 60 + q) for q in range(2)]
+    ds = [torch.from_numpy(p.view(np.int8)).cuda() for p in ps]
+    torch.cuda.synchronize()
+    ex = [oracle_mod.xengine_i64(oracle_mod.unpack4(p), n, f, t) for p in ps]
+    with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor", input_format="packed4") as c:
+        c.tune(1, 24, 1)
+        for q in (0, 1, 0, 1, 1):
+            c.run_device(ds[q].data_ptr(), xg.SYNCOP_NONE)
+        assert np.array_equal(c.dump_int64(), 2 * ex[0] + 3 * ex[1])
+        c.clear()
+        for q in (1, 0, 0):
+            c.run_device(ds[q].data_ptr(), xg.SYNCOP_NONE)
+        assert np.array_equal(c.dump_int64(), ex[1] + 2 * ex[0])
+
+
 def test_packed4_autotune_and_overlapping_device_calls(xg, oracle_mod):
     """Autotuning a packed context (its input buffers hold one byte per sample;
     the timing runs on its int8 conversion buffer), then several calls in

@@ -310,10 +310,10 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
   // Overlap with the previous launch only when nothing else sits between them
   // on the stream (no conversion, no copy to wait for) and that launch only
   // added into the buffer.
-  bool tail = in->adding_tail && in->s_comp == in->s_own && !input_ready &&
-              in->cfg.input_format == XGPU_INPUT_INT8;
-  in->adding_tail = false;
   const bool packed = packed_in_kernel(in);
+  bool tail = in->adding_tail && in->s_comp == in->s_own && !input_ready &&
+              (in->cfg.input_format == XGPU_INPUT_INT8 || packed);
+  in->adding_tail = false;
   if (in->cfg.input_format != XGPU_INPUT_INT8 && !packed) {
     conv = in->conv_cur;
     in->conv_cur ^= 1;
@@ -402,11 +402,12 @@ int dump(XGPUContext *ctx, Internal *in) {
 }
 
 // Channel groups for a dumping call over host buffers, 0 when the call goes
-// whole: int8 input only (a converted format is converted in one pass), at
-// least two groups of kGroupMinBytes, an output buffer that takes the dump.
+// whole: int8 input, or packed input that the CTA-pair kernel expands (a
+// converted format is converted in one pass), at least two groups of
+// kGroupMinBytes, an output buffer that takes the dump.
 int dump_groups(XGPUContext *ctx, Internal *in) {
   const Sizes &s = in->sz;
-  if (in->cfg.input_format != XGPU_INPUT_INT8 || s.f < 2) return 0;
+  if ((in->cfg.input_format != XGPU_INPUT_INT8 && !packed_in_kernel(in)) || s.f < 2) return 0;
   if (!in->matrix_h_set || !ctx->matrix_h) return 0;
   if (ctx->matrix_len && ctx->output_offset + (size_t)s.mat_length > ctx->matrix_len) return 0;
   long long g = s.input_bytes / kGroupMinBytes;
@@ -432,7 +433,10 @@ int dump_groups(XGPUContext *ctx, Internal *in) {
 int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
   const Sizes &s = in->sz;
   const int per = (s.f + groups - 1) / groups;
-  const size_t row = (size_t)s.n * kNpol * 2;   // bytes of one channel at one sample
+  const bool packed = packed_in_kernel(in);
+  // bytes of one channel at one sample: {re, im} bytes, or one packed byte,
+  // per station and polarisation
+  const size_t row = (size_t)s.n * kNpol * (packed ? 1 : 2);
   const size_t pitch = row * s.f;
   const char *src = (const char *)(ctx->array_h + ctx->input_offset);
   int8_t *dst = (int8_t *)in->d_in[b];
@@ -455,7 +459,7 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
     const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->group_in[k], 0));
     bool tail = false;
-    int r = launch_engine(in, dst, f0, fc, &tail);
+    int r = launch_engine(in, dst, f0, fc, &tail, packed);
     if (r != XGPU_OK) return r;
     if (direct) {
       XGPU_CHECK(cudaEventRecord(in->group_out[k], in->s_comp));
