@@ -92,8 +92,8 @@ struct Internal {
   // goes host-to-device while group k's results go device-to-host on s_dump
   // (the two directions' copy engines run at once).
   cudaStream_t s_dump = nullptr;
-  cudaEvent_t group_in[kMaxGroups] = {};    // a group's input is on the device
-  cudaEvent_t group_out[kMaxGroups] = {};   // a group's sums (or formatted results) are ready
+  cudaEvent_t group_in[kMaxGroups + 2] = {};    // a group's input is on the device
+  cudaEvent_t group_out[kMaxGroups + 2] = {};   // a group's sums (or formatted results) are ready
   cudaEvent_t copy_done[2] = {nullptr, nullptr};
   cudaEvent_t comp_done[2] = {nullptr, nullptr};
   int cur = 0;
@@ -197,7 +197,7 @@ int free_device(Internal *in) {
     cudaStreamSynchronize(in->s_dump);
     cudaStreamDestroy(in->s_dump);
   }
-  for (int k = 0; k < kMaxGroups; ++k) {
+  for (int k = 0; k < kMaxGroups + 2; ++k) {
     if (in->group_in[k]) cudaEventDestroy(in->group_in[k]);
     if (in->group_out[k]) cudaEventDestroy(in->group_out[k]);
   }
@@ -441,10 +441,29 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
   const char *src = (const char *)(ctx->array_h + ctx->input_offset);
   int8_t *dst = (int8_t *)in->d_in[b];
   in->adding_tail = false;
+  // Channel boundaries: the first and last groups hold half as many channels
+  // (at least one) as the others, so the first input copy and the last
+  // results -- the stretches in which only one direction of the host link
+  // is busy -- are short.  At most groups + 2 groups (2 <= 2 * half <= per
+  // <= f / 2).
+  int bound[kMaxGroups + 4];
+  int ng = 0;
+  {
+    const int half = per > 1 ? per / 2 : 1;
+    const int last0 = s.f - half;   // first channel of the last group
+    int f = half;
+    bound[0] = 0;
+    bound[++ng] = f;
+    while (f < last0) {
+      f = f + per < last0 ? f + per : last0;
+      bound[++ng] = f;
+    }
+    bound[++ng] = s.f;
+  }
   // The buffer is free once the engine launch that last read it has finished.
   XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
-  for (int k = 0; k < groups; ++k) {
-    const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
+  for (int k = 0; k < ng; ++k) {
+    const int f0 = bound[k], fc = bound[k + 1] - bound[k];
     XGPU_CHECK(cudaMemcpy2DAsync(dst + f0 * row, pitch, src + f0 * row, pitch, fc * row,
                                  (size_t)s.t, cudaMemcpyHostToDevice, in->s_copy));
     XGPU_CHECK(cudaEventRecord(in->group_in[k], in->s_copy));
@@ -455,8 +474,8 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
   // leave s_dump to the copies.
   void *direct = direct_output(ctx, in);
   cudaStream_t s_fmt = direct ? in->s_dump : in->s_comp;
-  for (int k = 0; k < groups; ++k) {
-    const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
+  for (int k = 0; k < ng; ++k) {
+    const int f0 = bound[k], fc = bound[k + 1] - bound[k];
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->group_in[k], 0));
     bool tail = false;
     int r = launch_engine(in, dst, f0, fc, &tail, packed);
@@ -479,8 +498,8 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
         planes ? (size_t)(s.mat_length / s.f) : (size_t)(2 * s.mat_length / s.f);
     char *host = (char *)(ctx->matrix_h + ctx->output_offset);
     const char *dev = (const char *)in->d_out;
-    for (int k = 0; k < groups; ++k) {
-      const int f0 = k * per, fc = s.f - f0 < per ? s.f - f0 : per;
+    for (int k = 0; k < ng; ++k) {
+      const int f0 = bound[k], fc = bound[k + 1] - bound[k];
       XGPU_CHECK(cudaStreamWaitEvent(in->s_dump, in->group_out[k], 0));
       for (int plane = 0; plane < (planes ? 2 : 1); ++plane) {
         const size_t off = ((size_t)plane * s.mat_length + (size_t)f0 * words) * 4;
@@ -636,7 +655,7 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
       cudaStreamCreateWithFlags(&in->s_dump, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&in->caller_ev, cudaEventDisableTiming) != cudaSuccess)
     return fail(XGPU_CUDA_ERROR);
-  for (int k = 0; k < kMaxGroups; ++k) {
+  for (int k = 0; k < kMaxGroups + 2; ++k) {
     if (cudaEventCreateWithFlags(&in->group_in[k], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&in->group_out[k], cudaEventDisableTiming) != cudaSuccess)
       return fail(XGPU_CUDA_ERROR);
