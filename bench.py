@@ -234,7 +234,7 @@ def float_output_error(xg, oracle, n, f, t, sigma, device):
             "zeros_exact": bool(not got[~nz].any())}
 
 
-def config4_shapes(seed=3, k=96):
+def uneven_subarray_shapes(seed=3, k=96):
     """96 subarrays: N log-uniform in [32,1024] rounded to 16, F uniform in
     [1,64], T a uniform multiple of 256 in [256,8192], sigma uniform in [4,32]."""
     import numpy as np
@@ -247,10 +247,10 @@ def config4_shapes(seed=3, k=96):
     return [(int(a), int(b_), int(c), float(d)) for a, b_, c, d in zip(n, f, t, sig)]
 
 
-def bench_config4(xg, torch, steps):
+def bench_uneven_batch(xg, torch, steps):
     """One persistent launch over 96 uneven subarrays (autotuned, CUDA graph)
     vs the same jobs run one by one on the tensor-core and plain engines."""
-    shapes = config4_shapes()
+    shapes = uneven_subarray_shapes()
     dev = torch.cuda.current_device()
     stream = torch.cuda.Stream()
     inputs, states, jobs = [], [], []
@@ -306,8 +306,9 @@ def bench_config4(xg, torch, steps):
     return out
 
 
-def config5_requests(seconds, seed=4, rate_jobs=200.0):
-    """Poisson arrivals of config-4-mix subarrays, each integrating 4-32 blocks."""
+def served_requests(seconds, seed=4, rate_jobs=200.0):
+    """Poisson arrivals of subarrays drawn like the 96-subarray batch, each
+    integrating 4-32 blocks."""
     import numpy as np
     rng = np.random.default_rng(seed)
     t, reqs = 0.0, []
@@ -326,13 +327,13 @@ def config5_requests(seconds, seed=4, rate_jobs=200.0):
 SAMPLE_RATE = 1.0e5   # per-channel complex samples/s of the served stream
 
 
-def bench_config5(xg, seconds, plain_seconds, device):
-    reqs = config5_requests(seconds)
+def bench_served_stream(xg, seconds, plain_seconds, device):
+    reqs = served_requests(seconds)
     st, _ = xg.serve(reqs, SAMPLE_RATE, 120 << 30, host_budget_bytes=24 << 30, device=device)
     out = {"arrival_rate_per_s": 200.0, "seconds": seconds, "sample_rate_hz": SAMPLE_RATE,
            "requests": len(reqs), "served": st}
     if plain_seconds > 0:
-        reqs_p = config5_requests(plain_seconds)
+        reqs_p = served_requests(plain_seconds)
         sp, _ = xg.serve(reqs_p, SAMPLE_RATE, 120 << 30, mode=xg.XGPU_SERVE_PLAIN_SERIAL,
                          host_budget_bytes=8 << 30, device=device)
         out["plain_serial"] = sp
@@ -340,7 +341,7 @@ def bench_config5(xg, seconds, plain_seconds, device):
     return out
 
 
-def bench_config3(xg, torch, device, blocks=64):
+def bench_large_array(xg, torch, device, blocks=64):
     """The large-array configuration: N=512, F=256, T=8192 per block, 64 blocks
     integrated before one dump, with packed 4+4-bit input expanded on the device
     (uniform [-7,7]) and an int8 variant (sigma 40).  Two distinct input blocks
@@ -507,7 +508,7 @@ def main():
     torch.cuda.set_device(local)
     clocks = Clocks(local)
 
-    # headline: tensor engine, config 2, input resident in HBM
+    # headline: tensor engine, xGPU's default shape, input resident in HBM
     ms, rot_bytes = device_engine_ms(xg, torch, "tensor", "int8", N, F, T, args.steps,
                                      args.warmup, world, tune=args.tune)
     ms = max_over_ranks(world, ms)
@@ -530,9 +531,9 @@ def main():
             detail[f"core_{kind}_peak_tops_measured"] = pk
             detail[f"plain_{kind}_n256_frac_of_core_peak"] = detail[f"plain_{kind}_n256_tops"] / pk
         if rank == 0:
-            # config 2 itself (every sum below 2^24: exact) and a long
+            # the default shape itself (every sum below 2^24: exact) and a long
             # integration whose sums pass 2^24
-            detail["float32_output_config2"] = float_output_error(xg, oracle, N, F, T, SIGMA, local)
+            detail["float32_output_n256_f10_t1024"] = float_output_error(xg, oracle, N, F, T, SIGMA, local)
             detail["float32_output_long"] = float_output_error(xg, oracle, 64, 10, 32768, 40.0,
                                                                local)
         k3 = max(3, min(args.steps, 10))
@@ -542,10 +543,10 @@ def main():
         detail["tc_n512_ms_per_block"] = ms3
         detail["tc_n512_tuning"] = TUNING.get(("tensor", N3, F3, T3))
         if rank == 0:
-            detail["config3_large_array"] = bench_config3(xg, torch, local)
-            detail["config4_batched"] = bench_config4(xg, torch, args.steps)
-            c5 = bench_config5(xg, args.serve_seconds, args.plain_serve_seconds, local)
-            detail["config5_served"] = c5
+            detail["large_array_n512_f256_t8192"] = bench_large_array(xg, torch, local)
+            detail["uneven_batch_96_subarrays"] = bench_uneven_batch(xg, torch, args.steps)
+            c5 = bench_served_stream(xg, args.serve_seconds, args.plain_serve_seconds, local)
+            detail["served_stream"] = c5
             detail["served_p50_dump_ms"] = c5["served"]["dump_p50_ms"]
             detail["served_p99_dump_ms"] = c5["served"]["dump_p99_ms"]
             detail["served_tops"] = c5["served"]["tops"]
