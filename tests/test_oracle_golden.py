@@ -119,3 +119,31 @@ def test_unpack4_roundtrip(oracle_mod):
     assert u.min() >= -7 and u.max() <= 7
     repacked = ((u[0::2].astype(np.int32) & 0xF) << 4) | (u[1::2].astype(np.int32) & 0xF)
     assert np.array_equal(repacked.astype(np.uint8), p.view(np.uint8))
+
+
+def test_scaled_packed_expansion_is_exact(oracle_mod):
+    """The arithmetic the CTA-pair kernel uses for packed input, restated on
+    the CPU: each nibble kept in (or moved to) the high half of its byte is 16
+    times its 4-bit value, so every sum of products is 256 times the true one
+    and an arithmetic shift by 8 recovers it exactly -- over every byte value,
+    including the nibble -8 (byte -128)."""
+    n, f, t = 16, 2, 256
+    rng = np.random.default_rng(5)
+    packed = rng.integers(0, 256, t * f * n * 2, dtype=np.uint8)
+    packed[:256] = np.arange(256, dtype=np.uint8)          # every value at least once
+    hi = (packed & 0xF0).view(np.int8).astype(np.int64)   # 16 x real part
+    lo = ((packed.astype(np.uint16) << 4) & 0xF0).astype(np.uint8).view(np.int8).astype(np.int64)
+    scaled = np.empty(packed.size * 2, dtype=np.int64)
+    scaled[0::2], scaled[1::2] = hi, lo
+    assert scaled.min() == -128 and scaled.max() == 112
+    exact = oracle_mod.xengine_i64(oracle_mod.unpack4(packed.view(np.int8)), n, f, t)
+    # the Gram formulation on the scaled bytes: x[t][f][s][p][c]
+    x = scaled.reshape(t, f, n, 2, 2)
+    re = np.einsum("tfip,tfjq->fijpq", x[..., 0], x[..., 0]) + \
+        np.einsum("tfip,tfjq->fijpq", x[..., 1], x[..., 1])
+    im = np.einsum("tfip,tfjq->fijpq", x[..., 1], x[..., 0]) - \
+        np.einsum("tfip,tfjq->fijpq", x[..., 0], x[..., 1])
+    assert not (re % 256).any() and not (im % 256).any()
+    i, j = np.tril_indices(n)
+    got = np.stack([re[:, i, j] >> 8, im[:, i, j] >> 8], axis=-1)   # [f][k][p][q][re,im]
+    assert np.array_equal(got.reshape(-1), exact)
