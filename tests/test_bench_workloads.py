@@ -1,0 +1,46 @@
+"""The bench's synthetic workloads, checked on the CPU: the 96-subarray batch
+and the served request stream are seeded draws with the stated ranges, and
+the same seed gives the same workload (so every run measures the same work)."""
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import bench  # noqa: E402
+
+
+def test_uneven_subarrays_are_seeded_and_in_range():
+    shapes = bench.uneven_subarray_shapes()
+    assert shapes == bench.uneven_subarray_shapes()
+    assert len(shapes) == 96
+    for n, f, t, sigma in shapes:
+        assert 32 <= n <= 1024 and n % 16 == 0
+        assert 1 <= f <= 64
+        assert 256 <= t <= 8192 and t % 256 == 0
+        assert 4.0 <= sigma <= 32.0
+    # log-uniform stations: both small and large arrays occur
+    ns = np.array([s[0] for s in shapes])
+    assert ns.min() < 64 and ns.max() > 512
+
+
+def test_served_requests_are_a_seeded_poisson_stream():
+    seconds, rate = 10.0, 200.0
+    reqs = bench.served_requests(seconds, rate_jobs=rate)
+    assert reqs == bench.served_requests(seconds, rate_jobs=rate)
+    arrivals = np.array([r["arrival_s"] for r in reqs])
+    assert (np.diff(arrivals) > 0).all() and arrivals[-1] <= seconds
+    # Poisson count: mean rate * seconds = 2000, standard deviation ~45
+    assert abs(len(reqs) - rate * seconds) < 5 * np.sqrt(rate * seconds)
+    for r in reqs:
+        assert 32 <= r["nstation"] <= 1024 and r["nstation"] % 16 == 0
+        assert 1 <= r["nfrequency"] <= 64
+        assert r["ntime"] % 256 == 0 and 256 <= r["ntime"] <= 8192
+        assert 4 <= r["nblocks"] <= 32
+    assert len({r["seed"] for r in reqs}) == len(reqs)
+
+
+def test_ops_formula_is_the_reference_flop_count():
+    # 16 F T N(N+1): 8 operations per complex multiply-add over N(N+1)/2
+    # baselines and 4 polarisation products (kernel.cuh:419)
+    assert bench.ops(256, 10, 1024) == 16 * 10 * 1024 * 256 * 257
