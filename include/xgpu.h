@@ -230,6 +230,17 @@ typedef struct XGPUConfigStruct {
   unsigned int matrix_order; /* TRIANGULAR_ORDER, REAL_IMAG_... or REGISTER_TILE_... */
   unsigned int engine;       /* XGPU_ENGINE_* */
   unsigned int input_format; /* XGPU_INPUT_* */
+  /* Channel range of a full-band input, for one context per GPU over one
+   * shared [t][f][s][p] buffer (xGPU selects the GPU with XGPU_DEVICE_MASK,
+   * xgpu.h:50, cuda_xengine.cu:193,225, but every context there reads a
+   * buffer of its own NFREQUENCY channels).  The input of one call holds
+   * input_nfrequency channels per sample; this context correlates channels
+   * [channel_offset, channel_offset + nfrequency) of it, in place, and its
+   * integration buffer and dumps hold those nfrequency channels only.
+   * input_nfrequency = 0 means nfrequency (the whole input, offset 0).
+   * xgpuContextInfo's vecLength is then the full-band input length. */
+  unsigned int channel_offset;
+  unsigned int input_nfrequency;
 } XGPUConfig;
 
 /* Fill cfg with this build's defaults (the sizes xgpuInfo reports). */
@@ -254,19 +265,23 @@ int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int sy
  * Integer engines only. */
 int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_out);
 
-/* Fill a device buffer with seeded synthetic samples, identical to the host
- * generator the tests use: kind 0 = Gaussian int8 with the given sigma,
- * rounded and clipped to [-127,127]; kind 1 = uniform integers in [-7,7] packed
- * 4+4-bit (one byte per complex sample); kind 2 = uniform int8 in [-7,7].
- * nbytes is the buffer size in bytes. */
+/* ---- Test and benchmark hooks (not part of xGPU's API; a correlator
+ * pipeline needs none of the three below) ---------------------------------- */
+
+/* Test and benchmark hook.  Fill a device buffer with seeded synthetic
+ * samples, identical to the host generator the tests use: kind 0 = Gaussian
+ * int8 with the given sigma, rounded and clipped to [-127,127]; kind 1 =
+ * uniform integers in [-7,7] packed 4+4-bit (one byte per complex sample);
+ * kind 2 = uniform int8 in [-7,7].  nbytes is the buffer size in bytes. */
 int xgpuGenerateDevice(void *device_out, size_t nbytes, int kind, unsigned long long seed,
                        double sigma, int device);
 
-/* Measure the device's CUDA-core rate for the plain engines' arithmetic (the
- * denominator of their rooflines) with a register-resident microbenchmark of
- * about 25 ms: kind 0 = dp4a, counted as 8 operations (four int8 products and
- * their sum), kind 1 = FP32 FMA, counted as 2.  *ops_per_second receives the
- * rate, in the X-engine's operations. */
+/* Benchmark hook.  Measure the device's CUDA-core rate for the plain
+ * engines' arithmetic (the denominator of their rooflines) with a
+ * register-resident microbenchmark of about 25 ms: kind 0 = dp4a, counted as
+ * 8 operations (four int8 products and their sum), kind 1 = FP32 FMA,
+ * counted as 2.  *ops_per_second receives the rate, in the X-engine's
+ * operations. */
 int xgpuMeasureCorePeak(int device, int kind, double *ops_per_second);
 
 /* Run the context's device work (engine launches, dump formatting) on the
@@ -295,11 +310,16 @@ void *xgpuComputeStream(XGPUContext *context);
  * The int64 integration buffer lives in a static 32 MiB device array that
  * every GPU loading the library holds until exit, so 64*F*N(N+1)/2 bytes must
  * fit in 32 MiB - 256 (e.g. N=256 with F <= 15); larger sizes return
- * XGPU_INVALID_ARGUMENT.  Work is queued on `stream` (a cudaStream_t, NULL for
- * the legacy default stream) and the call waits for it.  All calls share the
- * array: calls that overlap on the GPU race and must be serialised.  The
- * first call on a device looks up the array's device address, so make it
- * before any stream capture. */
+ * XGPU_INVALID_ARGUMENT, as do the sizes xgpuInitEx rejects and a channel
+ * range (channel_offset / input_nfrequency other than the whole input).  Work
+ * is queued on `stream` (a cudaStream_t, NULL for the legacy default stream)
+ * and the call waits for it and reads its error status back to the host, so
+ * it is synchronous and cannot be recorded into a CUDA graph.  The calling
+ * thread's current device is left as it was.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised.  The first call
+ * on a device looks up the array's device address and keeps it for the
+ * process's lifetime; after a cudaDeviceReset of that device the address is
+ * stale, so make no further call on it. */
 int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGPUConfig *cfg,
                         int device, void *stream);
 
@@ -322,7 +342,7 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);
  * autotuned choice and pass it to xgpuTune in a later run. */
 int xgpuTuning(XGPUContext *context, int *ksplit, int *grid, int *pair);
 
-/* Extension for testing a caller's error handling.  While enabled, the
+/* Test hook, for testing a caller's error handling.  While enabled, the
  * engine of this context (tensor-core or plain) issues no input loads, so its
  * bounded device waits expire (about 2 s per launch) instead of completing: the next
  * synchronising call returns XGPU_CUDA_ERROR, the integration in progress is

@@ -123,6 +123,38 @@ def test_check_result_reports(xg, capfd):
     assert "failed with 1 deviations" in capfd.readouterr().out
 
 
+def test_check_result_rounds_float_matrix_in_place(xg, capfd):
+    """xGPU's fixed-point float build rounds the GPU matrix in place before
+    comparing (cpu_util.c:164-167); the caller sees the rounded values."""
+    i = xg.default_info()
+    assert not xg.default_config().output_type == xg.XGPU_INT32   # float Complex build
+    cpu = np.zeros(i.triLength * 2, dtype=np.float32)
+    cpu[::7] = 1000.0
+    gpu = cpu + np.float32(0.375)
+    gpu[1::7] = -2.625
+    xg.lib().xgpuCheckResult(gpu.ctypes.data, cpu.ctypes.data, 0, None)
+    out = capfd.readouterr().out
+    assert np.array_equal(gpu, np.round(gpu))
+    assert gpu[0] == 1000.0 and gpu[1] == -3.0
+    assert "failed" in out       # the -3 entries deviate from zero
+
+
+def test_check_result_verbose_prints_samples_and_sum(xg, capfd):
+    i = xg.default_info()
+    n, f, t = i.nstation, i.nfrequency, i.ntime
+    cpu = np.zeros(i.triLength * 2, dtype=np.float32)
+    gpu = cpu.copy()
+    gpu[0] = 7.0      # f=0, baseline (0,0), pols (0,0), real part
+    x = np.zeros(t * f * n * 4, dtype=np.int8)
+    x[0], x[1] = 3, -2          # t=0, f=0, station 0, pol 0: 3 - 2i
+    xg.lib().xgpuCheckResult(gpu.ctypes.data, cpu.ctypes.data, 2, x.ctypes.data)
+    out = capfd.readouterr().out
+    assert "(   3,  -2) (   3,  -2) -> (    13,      0)" in out
+    lines = out.splitlines()
+    last = max(k for k, ln in enumerate(lines) if ln.startswith(f" {t - 1:4d} "))
+    assert lines[last + 1].strip() == "(    13,      0)"     # the sum after the samples
+
+
 def _ctx(xg):
     return xg.XGPUContext()
 
@@ -153,7 +185,7 @@ def test_core_peak_arguments_checked_before_any_device_call(xg):
 @pytest.mark.parametrize("field,value", [
     ("nstation", 24), ("nstation", 0), ("nfrequency", 0), ("ntimepipe", 8),
     ("ntime", 100), ("compute_type", 7), ("output_type", 0), ("matrix_order", 1234),
-    ("engine", 9), ("input_format", 5),
+    ("engine", 9), ("input_format", 5), ("ntime", 2**31 - 128), ("ntime", 2**32 - 128),
 ])
 def test_invalid_config_rejected_before_any_device_call(xg, field, value):
     cfg = xg.default_config()
@@ -185,3 +217,42 @@ def test_init_without_device_returns_error_not_exit(xg):
                          timeout=300)
     assert out.returncode == 0, out.stderr
     assert "RC 2 False" in out.stdout
+
+
+@pytest.mark.parametrize("offset,band,nfreq", [
+    (1, 0, 10),      # an offset needs the band's channel count
+    (3, 12, 10),     # range past the band's last channel
+    (0, 5, 10),      # band narrower than the range
+    (0, 70000, 10),  # band beyond the channel limit
+])
+def test_invalid_channel_range_rejected(xg, offset, band, nfreq):
+    cfg = xg.default_config()
+    cfg.nfrequency, cfg.channel_offset, cfg.input_nfrequency = nfreq, offset, band
+    ctx = _ctx(xg)
+    assert xg.lib().xgpuInitEx(ctypes.byref(ctx), 0, ctypes.byref(cfg)) == xg.XGPU_INVALID_ARGUMENT
+    assert not ctx.internal
+
+
+def _static_cfg(xg, n, f, t):
+    cfg = xg.default_config()
+    cfg.nstation, cfg.nfrequency, cfg.ntime, cfg.ntimepipe = n, f, t, 128
+    cfg.engine, cfg.input_format = xg.XGPU_ENGINE_TENSOR, xg.XGPU_INPUT_INT8
+    return cfg
+
+
+@pytest.mark.parametrize("change", [
+    {"nstation": 256, "nfrequency": 16},          # 64*F*N(N+1)/2 just past 32 MiB - 256
+    {"ntime": 2**31 - 128},                        # past the engines' sample count
+    {"channel_offset": 2, "input_nfrequency": 8},  # a channel range
+    {"input_nfrequency": 12},                      # input wider than the correlated channels
+    {"input_format": 1},                           # packed input
+])
+def test_static_entry_point_rejects_before_any_device_call(xg, change):
+    """xgpuCorrelateStatic checks every argument before touching a device:
+    the pointers below are never dereferenced."""
+    cfg = _static_cfg(xg, 256, 4, 1024)
+    for k, v in change.items():
+        setattr(cfg, k, v)
+    rc = xg.lib().xgpuCorrelateStatic(ctypes.c_void_p(1 << 20), ctypes.c_void_p(1 << 21),
+                                      ctypes.byref(cfg), 0, None)
+    assert rc == xg.XGPU_INVALID_ARGUMENT

@@ -1,0 +1,125 @@
+"""Contexts over channel ranges of one full-band input (XGPUConfig's
+channel_offset / input_nfrequency), the C-level form of sharding channels over
+GPUs: each GPU's context correlates its channels of the shared
+[t][f][s][p] buffer in place, with no re-packing by the caller.  xGPU has one
+context per device (XGPU_DEVICE_MASK, xgpu.h:50; cuda_xengine.cu:193,225),
+each over a buffer of its own.
+
+Channels are independent, so the triangular dumps of contexts over
+consecutive ranges, concatenated, must equal one context over the whole band,
+bit for bit (int32 and int64 dumps; float32 for the FP32 engine).  These run
+the ranges one after another on one GPU; on several GPUs each range's context
+would sit on its own device.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RANGES = [(0, 5), (5, 10)]
+
+
+def band_input(oracle_mod, fmt, n, f, t, seed):
+    """(feed in the context's input format, the int8 samples it holds)."""
+    if fmt == "packed4":
+        p = oracle_mod.generate(t * f * n * 2, 1, seed)
+        return p, oracle_mod.unpack4(p)
+    x = oracle_mod.gaussian_input(n, f, t, seed=seed, sigma=24.0)
+    if fmt == "dp4a_swizzled":
+        return oracle_mod.swizzle(x, n, f, t), x
+    if fmt == "block32":
+        return oracle_mod.block32(x), x
+    return x, x
+
+
+def ranged(xg, n, f0, f1, fband, t, **kw):
+    return xg.Correlator(n, f1 - f0, t, channel_offset=f0, input_nfrequency=fband, **kw)
+
+
+@pytest.mark.parametrize("engine,compute,tune", [
+    ("tensor", "int8", (1, 0, 0)), ("tensor", "int8", (1, 0, 1)), ("tensor", "int8", (2, 0, 1)),
+    ("plain", "int8", None), ("plain", "fp32", None)])
+@pytest.mark.parametrize("syncop", ["dump", "sync_compute"])
+def test_ranges_of_host_input_concatenate_to_the_band(xg, oracle_mod, engine, compute, tune,
+                                                      syncop):
+    """Host buffers: each context copies its channels of the band (a 2-D copy;
+    a dumping call in channel groups)."""
+    n, f, t = 256, 10, 1024
+    x = oracle_mod.gaussian_input(n, f, t, seed=31, sigma=20.0)
+    output = "int32" if compute == "int8" else "float32"
+    parts, parts64 = [], []
+    for f0, f1 in RANGES:
+        with ranged(xg, n, f0, f1, f, t, engine=engine, compute=compute, output=output,
+                    order="tri") as c:
+            assert c.info.vecLength == t * f * n * 2      # the caller's input is the band
+            assert c.info.triLength == (f1 - f0) * n * (n + 1) // 2 * 4
+            if tune:
+                c.tune(*tune)
+            c.set_input(x)
+            if syncop == "dump":
+                c.run(xg.SYNCOP_DUMP)
+                parts.append(c.output_view()[: c.info.matLength * 2].copy())
+            else:
+                c.run(xg.SYNCOP_SYNC_COMPUTE)
+                parts.append(c.dump())
+            if compute == "int8":
+                parts64.append(c.dump_int64())
+    got = xg.merge_triangular(parts)
+    if compute == "int8":
+        exact = oracle_mod.xengine_i64(x, n, f, t)
+        assert np.array_equal(xg.merge_triangular(parts64), exact)
+        assert np.array_equal(got, exact.astype(np.int32))
+    else:
+        assert np.array_equal(got, oracle_mod.xengine_f32(x, n, f, t))
+
+
+@pytest.mark.parametrize("fmt,tune", [("int8", (1, 0, 0)), ("int8", (1, 0, 1)),
+                                      ("packed4", (1, 0, 1)), ("packed4", (1, 0, 0)),
+                                      ("dp4a_swizzled", (1, 0, 0)), ("block32", (1, 0, 1))])
+def test_ranges_of_device_input_read_in_place(xg, oracle_mod, fmt, tune):
+    """Device-resident band: int8 (and packed input on CTA pairs) is read in
+    place through strided tensor maps; the other formats gather the range
+    before their conversion.  Two accumulating calls per context."""
+    import torch
+    n, f, t = 128, 7, 512
+    ranges = [(0, 3), (3, 4), (4, 7)]
+    feeds, xs = zip(*(band_input(oracle_mod, fmt, n, f, t, seed=40 + k) for k in range(2)))
+    devs = [torch.from_numpy(np.ascontiguousarray(q)).cuda() for q in feeds]
+    parts = []
+    for f0, f1 in ranges:
+        with ranged(xg, n, f0, f1, f, t, engine="tensor", input_format=fmt) as c:
+            c.tune(*tune)
+            c.run_device(devs[0].data_ptr(), xg.SYNCOP_NONE)
+            c.run_device(devs[1].data_ptr(), xg.SYNCOP_SYNC_COMPUTE)
+            parts.append(c.dump_int64())
+    want = oracle_mod.xengine_i64(np.concatenate(xs), n, f, 2 * t)
+    assert np.array_equal(xg.merge_triangular(parts), want)
+
+
+@pytest.mark.parametrize("fmt", ["packed4", "dp4a_swizzled", "block32"])
+def test_ranges_of_host_input_in_other_formats(xg, oracle_mod, fmt):
+    n, f, t = 64, 6, 512
+    feed, x = band_input(oracle_mod, fmt, n, f, t, seed=55)
+    parts = []
+    for f0, f1 in [(0, 1), (1, 4), (4, 6)]:
+        with ranged(xg, n, f0, f1, f, t, engine="tensor", input_format=fmt) as c:
+            c.set_input(feed)
+            c.run(xg.SYNCOP_DUMP)
+            parts.append(c.dump_int64())
+    assert np.array_equal(xg.merge_triangular(parts), oracle_mod.xengine_i64(x, n, f, t))
+
+
+def test_range_in_register_tile_order(xg, oracle_mod):
+    """The host input buffer holds the band; the dump of a range in
+    register-tile order is that range's own matrix."""
+    n, f, t = 64, 8, 256
+    x = oracle_mod.gaussian_input(n, f, t, seed=61)
+    with ranged(xg, n, 2, 7, f, t, engine="tensor", order="rt") as c:
+        view = c.input_view()
+        assert view.size == x.size
+        c.set_input(x)
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2]
+    sub = np.ascontiguousarray(x.reshape(t, f, n * 4)[:, 2:7, :]).reshape(-1)
+    exact = oracle_mod.xengine_i64(sub, n, 5, t)
+    assert np.array_equal(got, oracle_mod.tri_to_order(exact.astype(np.int32), n, 5, 3000))

@@ -54,6 +54,28 @@ def test_static_matches_context_path_twice(xg, oracle_mod):
         assert np.array_equal(got, want), (order, output)
 
 
+def test_static_at_the_size_limit(xg, oracle_mod):
+    """N=256 with F=15 fills the static array to within 256 bytes of its end
+    (64 * 15 * 32896 = 31,580,160 bytes <= 32 MiB - 256): accepted and equal
+    to the context path; F=16 (33,685,504 bytes) is rejected."""
+    import torch
+    n, t = 256, 256
+    x = oracle_mod.gaussian_input(n, 15, t, seed=151, sigma=30.0)
+    x_dev = torch.from_numpy(x).cuda()
+    want = context_result(xg, x_dev, n, 15, t, "tri", "int32")
+    got = static_result(xg, torch, x_dev, n, 15, t, "tri", "int32")
+    assert np.array_equal(got, want)
+    cfg = xg.default_config()
+    cfg.nstation, cfg.nfrequency, cfg.ntime, cfg.ntimepipe = n, 16, t, 128
+    cfg.engine, cfg.input_format = xg.XGPU_ENGINE_TENSOR, xg.XGPU_INPUT_INT8
+    big = torch.zeros(n * 16 * t * 4, dtype=torch.int8, device="cuda")
+    out = torch.zeros(16, dtype=torch.int32, device="cuda")
+    rc = xg.lib().xgpuCorrelateStatic(ctypes.c_void_p(big.data_ptr()),
+                                      ctypes.c_void_p(out.data_ptr()), ctypes.byref(cfg),
+                                      torch.cuda.current_device(), None)
+    assert rc == xg.XGPU_INVALID_ARGUMENT
+
+
 def test_static_rejects_sizes_beyond_the_array(xg):
     import torch
     cfg = xg.default_config()

@@ -117,6 +117,7 @@ class XGPUConfig(ctypes.Structure):
         ("ntimepipe", ctypes.c_uint), ("compute_type", ctypes.c_uint),
         ("output_type", ctypes.c_uint), ("matrix_order", ctypes.c_uint),
         ("engine", ctypes.c_uint), ("input_format", ctypes.c_uint),
+        ("channel_offset", ctypes.c_uint), ("input_nfrequency", ctypes.c_uint),
     ]
 
 
@@ -239,12 +240,15 @@ class Correlator:
 
     ``compute`` is "int8" (exact integer engines) or "fp32" (plain FP32),
     ``output`` the Complex member type ("int32" or "float32"), ``order`` one
-    of "tri", "ri", "rt", ``engine`` "tensor" or "plain".
+    of "tri", "ri", "rt", ``engine`` "tensor" or "plain".  With
+    ``input_nfrequency`` set, the input holds that many channels per sample
+    and the context correlates ``nfrequency`` of them from ``channel_offset``
+    on (XGPUConfig's channel range).
     """
 
     def __init__(self, nstation, nfrequency, ntime, ntimepipe=None, compute="int8",
                  output="int32", order="tri", engine="tensor", input_format="int8",
-                 device=0, flags=0):
+                 device=0, flags=0, channel_offset=0, input_nfrequency=0):
         cfg = default_config()
         cfg.nstation, cfg.nfrequency, cfg.ntime = nstation, nfrequency, ntime
         cfg.ntimepipe = ntimepipe if ntimepipe else min(ntime, 128)
@@ -253,6 +257,7 @@ class Correlator:
         cfg.matrix_order = ORDERS.get(order, order)
         cfg.engine = ENGINES.get(engine, engine)
         cfg.input_format = FORMATS.get(input_format, input_format)
+        cfg.channel_offset, cfg.input_nfrequency = channel_offset, input_nfrequency
         self.cfg = cfg
         self.ctx = XGPUContext()
         check("xgpuInitEx", lib().xgpuInitEx(ctypes.byref(self.ctx), device | flags,

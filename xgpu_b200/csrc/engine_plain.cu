@@ -5,7 +5,11 @@
 // shared_transfer_4_dp4a.cuh:99-164).  The arithmetic per thread is the same:
 // each thread owns a 2x2 block of stations (rows i, i+1 x columns j, j+1) and
 // all 4 polarisation products of each, i.e. 16 complex visibilities.
-//   FP32: 32 float accumulators, 64 FMAs per sample.
+//   FP32: 32 float accumulators; per sample and visibility the two products
+//         of the real (and of the imaginary) part are summed exactly and the
+//         sum is added with one rounding, as xGPU's float engine does
+//         (omp_xengine.c:24-28), so the sums equal its own bit for bit:
+//         3 FP32 instructions per component, 96 per sample.
 //   dp4a: 48 int32 accumulators (re, im1, im2 as in kernel.cuh:464-479,574),
 //         64 dp4a per group of 4 samples.
 // What changes is the data path.  xGPU fetches one sample at a time through
@@ -256,12 +260,27 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int nchunks = (p.tcount + kTcF - 1) / kTcF;
 
+  // The accumulators continue the integration buffer's sums (0 after a
+  // clear), so an integration over several calls is one sum in time order.
   float sr[2][2][2][2], si[2][2][2][2];
+  float *state = (float *)p.state;
 #pragma unroll
-  for (int a = 0; a < 16; ++a) {
-    (&sr[0][0][0][0])[a] = 0.f;
-    (&si[0][0][0][0])[a] = 0.f;
-  }
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 2; ++cs) {
+      const int i = rb * kBlk + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
+      const bool mine = !p.overwrite && i < p.n && j <= i;
+      const float4 *src = (const float4 *)(state + ((long long)f * p.nbaseline +
+                                                    (long long)i * (i + 1) / 2 + j) * 8);
+#pragma unroll
+      for (int p1 = 0; p1 < 2; ++p1) {
+        const float4 o = mine ? src[p1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        sr[rs][cs][p1][0] = o.x;
+        si[rs][cs][p1][0] = o.y;
+        sr[rs][cs][p1][1] = o.z;
+        si[rs][cs][p1][1] = o.w;
+      }
+    }
 
   const uint32_t bar0 = tc::smem_u32(&bars[0]);
   if (threadIdx.x == 0) {
@@ -302,23 +321,24 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
         for (int cs = 0; cs < 2; ++cs) {
           const float ar[2] = {r[rs].x, r[rs].z}, ai[2] = {r[rs].y, r[rs].w};
           const float br[2] = {c[cs].x, c[cs].z}, bi[2] = {c[cs].y, c[cs].w};
+          // xGPU's float arithmetic (omp_xengine.c:24-28): a sample's
+          // two products are summed first -- exactly: products of int8
+          // values and their sums are integers below 2^24 -- and the sum is
+          // added to the accumulator with one rounding.
 #pragma unroll
           for (int p1 = 0; p1 < 2; ++p1)
 #pragma unroll
             for (int p2 = 0; p2 < 2; ++p2) {
               float &x = sr[rs][cs][p1][p2];
               float &y = si[rs][cs][p1][p2];
-              x = fmaf(ar[p1], br[p2], x);
-              x = fmaf(ai[p1], bi[p2], x);
-              y = fmaf(ai[p1], br[p2], y);
-              y = fmaf(-ar[p1], bi[p2], y);
+              x = __fadd_rn(x, __fmaf_rn(ai[p1], bi[p2], __fmul_rn(ar[p1], br[p2])));
+              y = __fadd_rn(y, __fmaf_rn(ai[p1], br[p2], -__fmul_rn(ar[p1], bi[p2])));
             }
         }
     }
     __syncthreads();
   }
 
-  float *state = (float *)p.state;
 #pragma unroll
   for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
@@ -328,18 +348,9 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
       float4 *dst = (float4 *)(state + ((long long)f * p.nbaseline +
                                         (long long)i * (i + 1) / 2 + j) * 8);
 #pragma unroll
-      for (int p1 = 0; p1 < 2; ++p1) {
-        float4 v = make_float4(sr[rs][cs][p1][0], si[rs][cs][p1][0], sr[rs][cs][p1][1],
-                               si[rs][cs][p1][1]);
-        if (!p.overwrite) {
-          const float4 o = dst[p1];
-          v.x += o.x;
-          v.y += o.y;
-          v.z += o.z;
-          v.w += o.w;
-        }
-        dst[p1] = v;
-      }
+      for (int p1 = 0; p1 < 2; ++p1)
+        dst[p1] = make_float4(sr[rs][cs][p1][0], si[rs][cs][p1][0], sr[rs][cs][p1][1],
+                              si[rs][cs][p1][1]);
     }
 }
 

@@ -430,15 +430,16 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return encode;
 }
 
-// {x: 4n bytes, y: f, z: t} over [t][f][s][p][c] int8 input; boxes of
-// 128 bytes (32 stations) x `rows` samples.
+// {x: 4n bytes, y: f, z: t} over [t][f][s][p][c] int8 input with s.fin
+// channels per sample (the map covers f of them); boxes of 128 bytes (32
+// stations) x `rows` samples.
 static int input_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int rows,
                      CUtensorMapSwizzle swizzle) {
   const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (!encode) return -1;
-  if (((uintptr_t)dev_in & 15) != 0) return -2;
+  if (((uintptr_t)dev_in & 15) != 0 || s.fin < s.f) return -2;
   cuuint64_t dims[3] = {(cuuint64_t)4 * s.n, (cuuint64_t)s.f, (cuuint64_t)s.t};
-  cuuint64_t strides[2] = {(cuuint64_t)4 * s.n, (cuuint64_t)4 * s.n * s.f};
+  cuuint64_t strides[2] = {(cuuint64_t)4 * s.n, (cuuint64_t)4 * s.n * s.fin};
   cuuint32_t box[3] = {(cuuint32_t)tc::kTile, 1, (cuuint32_t)rows};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(dev_in), dims,
@@ -458,9 +459,9 @@ int make_panel_map(CUtensorMap *map, const void *dev_in, const Sizes &s, int row
 int make_packed_map(CUtensorMap *map, const void *dev_in, const Sizes &s) {
   const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (!encode) return -1;
-  if (((uintptr_t)dev_in & 15) != 0 || s.n % 8 != 0) return -2;
+  if (((uintptr_t)dev_in & 15) != 0 || s.n % 8 != 0 || s.fin < s.f) return -2;
   cuuint64_t dims[3] = {(cuuint64_t)2 * s.n, (cuuint64_t)s.f, (cuuint64_t)s.t};
-  cuuint64_t strides[2] = {(cuuint64_t)2 * s.n, (cuuint64_t)2 * s.n * s.f};
+  cuuint64_t strides[2] = {(cuuint64_t)2 * s.n, (cuuint64_t)2 * s.n * s.fin};
   cuuint32_t box[3] = {(cuuint32_t)tc::kTile / 2, 1, (cuuint32_t)tc::kKt};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(dev_in), dims,

@@ -96,15 +96,18 @@ void xgpuReorderMatrix(Complex *matrix) {
 }
 
 // Relative complex error check with xGPU's tolerances and report
-// (cpu_util.c:134-232): 1e-5 for fixed-point input; GPU values are rounded
-// first when the output is float.
+// (cpu_util.c:134-232): 1e-5 for fixed-point input.  When the output is float
+// (xGPU's FIXED_POINT build without DP4A) the GPU matrix is rounded to
+// integers in place first, as xGPU does (cpu_util.c:164-167): callers see the
+// rounded values afterwards.
 void xgpuCheckResult(Complex *gpu, Complex *cpu, int verbose, ComplexInput *array_h) {
   const XGPUInfo in = defaults();
   const bool is_int = int_words();
   const double tol = 1e-5;
   printf("Checking result (tolerance == %g)...\n", tol);
   fflush(stdout);
-  const uint32_t *g = (const uint32_t *)gpu, *c = (const uint32_t *)cpu;
+  uint32_t *g = (uint32_t *)gpu;
+  const uint32_t *c = (const uint32_t *)cpu;
   const long long n = in.nstation, nf = in.nfrequency;
   long long errors = 0;
   double max_err = 0.0;
@@ -120,6 +123,9 @@ void xgpuCheckResult(Complex *gpu, Complex *cpu, int verbose, ComplexInput *arra
             if (!is_int) {
               gr = round(gr);
               gi = round(gi);
+              const float fr = (float)gr, fi = (float)gi;
+              memcpy(&g[2 * idx], &fr, 4);
+              memcpy(&g[2 * idx + 1], &fi, 4);
             }
             const double cabs = sqrt(cr * cr + ci * ci);
             const double dr = cr - gr, di = ci - gi;
@@ -132,12 +138,19 @@ void xgpuCheckResult(Complex *gpu, Complex *cpu, int verbose, ComplexInput *arra
                 printf("%3lld %3lld %3lld %4lld %2d %2d %5lld %12g  %12g  %12g  %12g\n", f, i, j, k, p1,
                        p2, idx, cr, gr, ci, gi);
                 if (verbose > 1 && array_h) {
+                  long long sr = 0, si = 0;
                   for (long long t = 0; t < (long long)in.ntime; t++) {
                     const ComplexInput a = array_h[((t * nf + f) * n + i) * 2 + p1];
                     const ComplexInput b = array_h[((t * nf + f) * n + j) * 2 + p2];
+                    const int pr = a.real * b.real + a.imag * b.imag;
+                    const int pi = a.imag * b.real - a.real * b.imag;
+                    sr += pr;
+                    si += pi;
                     printf(" %4lld (%4d,%4d) (%4d,%4d) -> (%6d, %6d)\n", t, a.real, a.imag, b.real,
-                           b.imag, a.real * b.real + a.imag * b.imag, a.imag * b.real - a.real * b.imag);
+                           b.imag, pr, pi);
                   }
+                  // the per-sample products' sum, as xGPU prints it
+                  printf("                                 (%6lld, %6lld)\n", sr, si);
                 }
               }
               errors++;

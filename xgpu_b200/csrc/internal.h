@@ -40,9 +40,28 @@ struct Sizes {
   long long mat_length;  // Complex elements of a dump in the context's order
   long long tri_length;  // Complex elements in triangular order
   long long state_elems; // int64 (or float) words of the integration buffer = tri_length*2
+  // Input geometry.  The engines' tensor maps step fin channels per sample
+  // (fin == f for a compact buffer of this context's channels; the full band
+  // when a context of a channel range reads the caller's input in place, from
+  // channel fin0 on).
+  int fin;               // channels per sample of the input the maps describe
+  int fin0;              // first correlated channel of a full-band input
+  int fband;             // channels per sample of the caller's input (cfg.input_nfrequency)
+  long long band_bytes;  // bytes of one call's full-band input in its format
+  long long chan_bytes;  // bytes of one channel in one row of the input (see rows)
+  long long rows;        // rows of the input: samples, or 4-sample groups (DP4A swizzle)
 };
 
 Sizes make_sizes(const XGPUConfig &cfg);
+// 1 if cfg is within the documented ranges of xgpuInitEx (channel range included).
+int validate_config(const XGPUConfig &cfg);
+// The same sizes with the input read as a compact buffer of this context's
+// channels (fin = f, fin0 = 0).
+inline Sizes compact_sizes(Sizes s) {
+  s.fin = s.f;
+  s.fin0 = 0;
+  return s;
+}
 
 // ---- engines --------------------------------------------------------------
 // All engines read int8 input laid out [t][f][s][p][c] (t = 0..t_total) and
@@ -96,7 +115,8 @@ int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount
 cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
                              int grid, cudaStream_t st, int max_item_steps);
 // Encodes the 3-D tensor map {x: 4n bytes, y: f, z: t} over a device input
-// buffer.  Returns 0 on success.
+// buffer whose samples are s.fin channels apart (dev_in points at the first
+// channel the map covers).  Returns 0 on success.
 int make_tc_tensor_map(CUtensorMap *map, const void *dev_in, const Sizes &s);
 // The same map with unswizzled boxes of 128 bytes x `rows` samples (the plain
 // engines' panels).

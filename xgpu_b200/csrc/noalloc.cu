@@ -25,7 +25,12 @@
 // In host code `g_noalloc_scratch` is only a host-side stand-in for the
 // device array: its device address comes from cudaGetSymbolAddress, taken
 // once per device with that device current, on the first call made on that
-// device.  That first call should therefore come before any stream capture.
+// device, and kept for the life of the process (a cudaDeviceReset of that
+// device invalidates it: make no call on a device after resetting it).
+//
+// Every call waits for its own work (cudaStreamSynchronize) and reads the
+// error word back into host memory, so a call cannot be recorded into a CUDA
+// graph.  The caller's current device is the same after the call as before.
 #include <string.h>
 
 #include <mutex>
@@ -61,6 +66,9 @@ void *scratch_on(int device) {
   return g_scratch_addr[device];
 }
 
+int correlate_static(const void *device_input, void *device_output, const XGPUConfig &c,
+                     const Sizes &s, int device, void *stream);
+
 }  // namespace
 
 extern "C" int xgpuCorrelateStatic(const void *device_input, void *device_output,
@@ -69,16 +77,14 @@ extern "C" int xgpuCorrelateStatic(const void *device_input, void *device_output
   if (((uintptr_t)device_input & 15) != 0 || ((uintptr_t)device_output & 7) != 0)
     return XGPU_INVALID_ARGUMENT;
   if (device < 0 || device >= kMaxDevices) return XGPU_INVALID_ARGUMENT;
-  const XGPUConfig &c = *cfg;
-  if (c.nstation < 16 || c.nstation % 16 != 0 || c.nfrequency < 1 || c.ntimepipe < 16 ||
-      c.ntimepipe % 16 != 0 || c.ntime < c.ntimepipe || c.ntime % c.ntimepipe != 0)
-    return XGPU_INVALID_ARGUMENT;
+  XGPUConfig c = *cfg;
+  if (c.engine == XGPU_ENGINE_DEFAULT) c.engine = XGPU_ENGINE_TENSOR;
+  // xgpuInitEx's ranges (sample count included), then this path's own limits:
+  // the tensor-core engine on int8 input covering the whole buffer
+  if (!validate_config(c)) return XGPU_INVALID_ARGUMENT;
   if (c.compute_type != XGPU_INT8 || c.input_format != XGPU_INPUT_INT8 ||
-      (c.engine != XGPU_ENGINE_TENSOR && c.engine != XGPU_ENGINE_DEFAULT))
-    return XGPU_INVALID_ARGUMENT;
-  if (c.output_type != XGPU_INT32 && c.output_type != XGPU_FLOAT32) return XGPU_INVALID_ARGUMENT;
-  if (c.matrix_order != TRIANGULAR_ORDER && c.matrix_order != REAL_IMAG_TRIANGULAR_ORDER &&
-      c.matrix_order != REGISTER_TILE_TRIANGULAR_ORDER)
+      c.engine != XGPU_ENGINE_TENSOR || c.channel_offset != 0 ||
+      (c.input_nfrequency != 0 && c.input_nfrequency != c.nfrequency))
     return XGPU_INVALID_ARGUMENT;
 
   const Sizes s = make_sizes(c);
@@ -91,7 +97,19 @@ extern "C" int xgpuCorrelateStatic(const void *device_input, void *device_output
     return XGPU_INVALID_ARGUMENT;
   }
 
+  int caller_device = 0;
+  if (cudaGetDevice(&caller_device) != cudaSuccess) return XGPU_CUDA_ERROR;
   if (cudaSetDevice(device) != cudaSuccess) return XGPU_CUDA_ERROR;
+  const int rc = correlate_static(device_input, device_output, c, s, device, stream);
+  cudaSetDevice(caller_device);
+  return rc;
+}
+
+namespace {
+
+// The body of xgpuCorrelateStatic with `device` current.
+int correlate_static(const void *device_input, void *device_output, const XGPUConfig &c,
+                     const Sizes &s, int device, void *stream) {
   unsigned char *base = (unsigned char *)scratch_on(device);
   if (!base) return XGPU_CUDA_ERROR;
   int *err = (int *)base;
@@ -119,3 +137,5 @@ extern "C" int xgpuCorrelateStatic(const void *device_input, void *device_output
   }
   return XGPU_OK;
 }
+
+}  // namespace

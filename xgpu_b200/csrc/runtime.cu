@@ -64,7 +64,8 @@ constexpr long long kGroupMinBytes = 1 << 20;
 struct Internal {
   int device = 0;
   XGPUConfig cfg{};
-  Sizes sz{};
+  Sizes sz{};    // the context's sizes; input geometry of the caller's full-band device input
+  Sizes szc{};   // the same for a compact copy of this context's channels (d_in, d_conv)
   bool int_state = true;  // int64 buffer (integer engines) or float (FP32)
 
   void *d_in[2] = {nullptr, nullptr};  // one call's input, as supplied
@@ -81,6 +82,9 @@ struct Internal {
   bool conv_used[2] = {false, false};
   int conv_cur = 0;
   cudaEvent_t caller_ev = nullptr;                 // orders caller-stream work before a conversion
+  // A context of a channel range with a converted format gathers its channels
+  // of device-resident input here (on s_conv) before converting them.
+  void *d_slice = nullptr;
   void *d_state = nullptr;             // integration buffer
   void *d_out = nullptr;               // formatted dump
   int *d_err = nullptr;                // device error word
@@ -108,6 +112,7 @@ struct Internal {
   struct MapEntry {
     const void *ptr;
     bool packed;     // packed 4+4-bit geometry (make_packed_map)
+    int fin;         // channels per sample of the buffer
     CUtensorMap map;
   } maps[4];
   int nmaps = 0;
@@ -142,26 +147,9 @@ XGPUConfig default_config() {
   c.matrix_order = XGPU_DEFAULT_ORDER;
   c.engine = XGPU_ENGINE_TENSOR;
   c.input_format = XGPU_INPUT_INT8;
+  c.channel_offset = 0;
+  c.input_nfrequency = 0;
   return c;
-}
-
-int validate(const XGPUConfig &c) {
-  if (c.nstation < 16 || c.nstation % 16 != 0 || c.nstation > 8192) return 0;
-  if (c.nfrequency < 1 || c.nfrequency > 65535) return 0;
-  if (c.ntimepipe < 16 || c.ntimepipe % 16 != 0) return 0;
-  if (c.ntime < c.ntimepipe || c.ntime % c.ntimepipe != 0) return 0;
-  if (c.compute_type != XGPU_INT8 && c.compute_type != XGPU_FLOAT32) return 0;
-  if (c.output_type != XGPU_INT32 && c.output_type != XGPU_FLOAT32) return 0;
-  if (c.matrix_order != TRIANGULAR_ORDER && c.matrix_order != REAL_IMAG_TRIANGULAR_ORDER &&
-      c.matrix_order != REGISTER_TILE_TRIANGULAR_ORDER)
-    return 0;
-  if (c.engine > XGPU_ENGINE_TENSOR) return 0;
-  if (c.engine == XGPU_ENGINE_TENSOR && c.compute_type != XGPU_INT8) return 0;
-  if (c.input_format > XGPU_INPUT_BLOCK32) return 0;
-  // input bytes of one call must fit the 32-bit sample index space of the engines
-  const double bytes = 4.0 * c.nstation * c.nfrequency * (double)c.ntime;
-  if (bytes > 1.0e12) return 0;
-  return 1;
 }
 
 void fill_info(const XGPUConfig &c, const Sizes &s, XGPUInfo *info) {
@@ -173,8 +161,9 @@ void fill_info(const XGPUConfig &c, const Sizes &s, XGPUInfo *info) {
   info->ntimepipe = c.ntimepipe;
   info->input_type = XGPU_INT8;
   info->compute_type = c.compute_type;
-  info->vecLength = (unsigned long long)s.vec_length;
-  info->vecLengthPipe = (unsigned long long)c.nfrequency * c.ntimepipe * c.nstation * kNpol;
+  // the caller's input holds the whole band (s.fband channels)
+  info->vecLength = (unsigned long long)s.t * s.fband * s.n * kNpol;
+  info->vecLengthPipe = (unsigned long long)s.fband * c.ntimepipe * c.nstation * kNpol;
   info->matLength = (unsigned long long)s.mat_length;
   info->triLength = (unsigned long long)s.tri_length;
   info->matrix_order = c.matrix_order;
@@ -211,6 +200,7 @@ int free_device(Internal *in) {
     cudaStreamDestroy(in->s_conv);
   }
   if (in->caller_ev) cudaEventDestroy(in->caller_ev);
+  if (in->d_slice) cudaFree(in->d_slice);
   if (in->d_state) cudaFree(in->d_state);
   if (in->d_out) cudaFree(in->d_out);
   if (in->d_err) cudaFree(in->d_err);
@@ -241,18 +231,21 @@ cudaError_t register_range(void *p, size_t bytes, void **registered) {
   return e;
 }
 
-const CUtensorMap *tensor_map(Internal *in, const void *ptr, bool packed = false) {
+// Tensor map over input at ptr with geometry g (g.fin channels per sample).
+const CUtensorMap *tensor_map(Internal *in, const void *ptr, const Sizes &g, bool packed = false) {
   for (int q = 0; q < in->nmaps; ++q)
-    if (in->maps[q].ptr == ptr && in->maps[q].packed == packed) return &in->maps[q].map;
+    if (in->maps[q].ptr == ptr && in->maps[q].packed == packed && in->maps[q].fin == g.fin)
+      return &in->maps[q].map;
   const int slot = in->nmaps < 4 ? in->nmaps++ : 3;
-  const int r = packed ? make_packed_map(&in->maps[slot].map, ptr, in->sz)
-                       : make_tc_tensor_map(&in->maps[slot].map, ptr, in->sz);
+  const int r = packed ? make_packed_map(&in->maps[slot].map, ptr, g)
+                       : make_tc_tensor_map(&in->maps[slot].map, ptr, g);
   if (r != 0) {
     in->maps[slot].ptr = nullptr;
     return nullptr;
   }
   in->maps[slot].ptr = ptr;
   in->maps[slot].packed = packed;
+  in->maps[slot].fin = g.fin;
   return &in->maps[slot].map;
 }
 
@@ -266,12 +259,13 @@ bool packed_in_kernel(const Internal *in) {
 
 // Queue the engine over channels [f0, f0 + fcount) of int8 input x (packed
 // input when `packed`: packed_in_kernel) on s_comp, in time segments; the
-// first segment stores when the buffer is known to be zero.  *tail: in, the
-// launch may overlap the adding launch before it; out, the last launch queued
-// only added.
-int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail,
+// first segment stores when the buffer is known to be zero.  x has geometry s
+// (in->szc for the context's compact buffers, in->sz for a full-band device
+// input read in place, x then pointing at the context's first channel).
+// *tail: in, the launch may overlap the adding launch before it; out, the
+// last launch queued only added.
+int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fcount, bool *tail,
                   bool packed = false) {
-  const Sizes &s = in->sz;
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
     XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
@@ -283,7 +277,7 @@ int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail,
                                    in->s_comp, in->d_err, in->tune.stall, f0, fcount));
     }
   } else {
-    const CUtensorMap *map = tensor_map(in, x, packed);
+    const CUtensorMap *map = tensor_map(in, x, s, packed);
     if (!map) {
       fprintf(stderr, "xgpu: cannot describe the input buffer to the tensor memory accelerator\n");
       return XGPU_CUDA_ERROR;
@@ -303,9 +297,15 @@ int launch_engine(Internal *in, const int8_t *x, int f0, int fcount, bool *tail,
 // Queue the engine over one call's device input (any format) on s_comp.
 // input_ready, when given, is the event after which the input is complete
 // (the host-to-device copy); converted formats wait for it on s_conv.
-int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
+// compact: d_input holds only this context's channels (the copy the host path
+// makes); otherwise it is the caller's full-band input, read in place (int8,
+// or packed input the CTA-pair kernel expands) or gathered into d_slice
+// before its conversion (the other formats).
+int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready, bool compact) {
   const Sizes &s = in->sz;
+  const bool ranged = !compact && s.fin != s.f;
   const int8_t *x = (const int8_t *)d_input;
+  const Sizes *geom = &in->szc;
   int conv = -1;
   // Overlap with the previous launch only when nothing else sits between them
   // on the stream (no conversion, no copy to wait for) and that launch only
@@ -324,20 +324,33 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready) {
       XGPU_CHECK(cudaEventRecord(in->caller_ev, in->s_comp));
       XGPU_CHECK(cudaStreamWaitEvent(in->s_conv, in->caller_ev, 0));
     }
+    const void *src = d_input;
+    if (ranged) {
+      // this context's channels of every row of the band, gathered in order
+      XGPU_CHECK(cudaMemcpy2DAsync(in->d_slice, (size_t)(s.f * s.chan_bytes),
+                                   (const char *)d_input + s.fin0 * s.chan_bytes,
+                                   (size_t)(s.fband * s.chan_bytes), (size_t)(s.f * s.chan_bytes),
+                                   (size_t)s.rows, cudaMemcpyDeviceToDevice, in->s_conv));
+      src = in->d_slice;
+    }
     if (in->cfg.input_format == XGPU_INPUT_PACKED4)
-      XGPU_CHECK(launch_unpack4((const uint8_t *)d_input, in->d_conv[conv], s.vec_length, in->s_conv));
+      XGPU_CHECK(launch_unpack4((const uint8_t *)src, in->d_conv[conv], s.vec_length, in->s_conv));
     else if (in->cfg.input_format == XGPU_INPUT_BLOCK32)
-      XGPU_CHECK(launch_unblock32((const int8_t *)d_input, in->d_conv[conv], 2 * s.vec_length,
+      XGPU_CHECK(launch_unblock32((const int8_t *)src, in->d_conv[conv], 2 * s.vec_length,
                                   in->s_conv));
     else
-      XGPU_CHECK(launch_unswizzle_dp4a((const int8_t *)d_input, in->d_conv[conv], s, in->s_conv));
+      XGPU_CHECK(launch_unswizzle_dp4a((const int8_t *)src, in->d_conv[conv], in->szc, in->s_conv));
     XGPU_CHECK(cudaEventRecord(in->conv_done[conv], in->s_conv));
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->conv_done[conv], 0));
     x = in->d_conv[conv];
-  } else if (input_ready) {
-    XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, input_ready, 0));
+  } else {
+    if (input_ready) XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, input_ready, 0));
+    if (ranged) {
+      x += s.fin0 * s.chan_bytes;   // the maps step the band's fin channels per sample
+      geom = &in->sz;
+    }
   }
-  const int r = launch_engine(in, x, 0, s.f, &tail, packed);
+  const int r = launch_engine(in, x, *geom, 0, s.f, &tail, packed);
   if (r != XGPU_OK) return r;
   if (in->int_state && in->cfg.engine == XGPU_ENGINE_TENSOR) in->adding_tail = tail && conv < 0;
   in->state_zero = false;
@@ -435,10 +448,11 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
   const int per = (s.f + groups - 1) / groups;
   const bool packed = packed_in_kernel(in);
   // bytes of one channel at one sample: {re, im} bytes, or one packed byte,
-  // per station and polarisation
-  const size_t row = (size_t)s.n * kNpol * (packed ? 1 : 2);
-  const size_t pitch = row * s.f;
-  const char *src = (const char *)(ctx->array_h + ctx->input_offset);
+  // per station and polarisation; the host rows hold the whole band, the
+  // device copy this context's channels
+  const size_t row = (size_t)s.chan_bytes;
+  const size_t pitch = row * s.f, src_pitch = row * s.fband;
+  const char *src = (const char *)(ctx->array_h + ctx->input_offset) + (size_t)s.fin0 * row;
   int8_t *dst = (int8_t *)in->d_in[b];
   in->adding_tail = false;
   // Channel boundaries: the first and last groups hold half as many channels
@@ -464,8 +478,8 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
   XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
   for (int k = 0; k < ng; ++k) {
     const int f0 = bound[k], fc = bound[k + 1] - bound[k];
-    XGPU_CHECK(cudaMemcpy2DAsync(dst + f0 * row, pitch, src + f0 * row, pitch, fc * row,
-                                 (size_t)s.t, cudaMemcpyHostToDevice, in->s_copy));
+    XGPU_CHECK(cudaMemcpy2DAsync(dst + f0 * row, pitch, src + f0 * row, src_pitch, fc * row,
+                                 (size_t)s.rows, cudaMemcpyHostToDevice, in->s_copy));
     XGPU_CHECK(cudaEventRecord(in->group_in[k], in->s_copy));
   }
   XGPU_CHECK(cudaEventRecord(in->copy_done[b], in->s_copy));
@@ -478,7 +492,7 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
     const int f0 = bound[k], fc = bound[k + 1] - bound[k];
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->group_in[k], 0));
     bool tail = false;
-    int r = launch_engine(in, dst, f0, fc, &tail, packed);
+    int r = launch_engine(in, dst, in->szc, f0, fc, &tail, packed);
     if (r != XGPU_OK) return r;
     if (direct) {
       XGPU_CHECK(cudaEventRecord(in->group_out[k], in->s_comp));
@@ -531,6 +545,31 @@ int finish_call(XGPUContext *ctx, Internal *in, int syncOp) {
 
 namespace xgpu {
 
+int validate_config(const XGPUConfig &c) {
+  if (c.nstation < 16 || c.nstation % 16 != 0 || c.nstation > 8192) return 0;
+  if (c.nfrequency < 1 || c.nfrequency > 65535) return 0;
+  if (c.ntimepipe < 16 || c.ntimepipe % 16 != 0) return 0;
+  if (c.ntime < c.ntimepipe || c.ntime % c.ntimepipe != 0) return 0;
+  // the engines count samples in int and step through them kSegment at a time
+  if (c.ntime > 0x7fffffffu - (unsigned)kSegment) return 0;
+  if (c.compute_type != XGPU_INT8 && c.compute_type != XGPU_FLOAT32) return 0;
+  if (c.output_type != XGPU_INT32 && c.output_type != XGPU_FLOAT32) return 0;
+  if (c.matrix_order != TRIANGULAR_ORDER && c.matrix_order != REAL_IMAG_TRIANGULAR_ORDER &&
+      c.matrix_order != REGISTER_TILE_TRIANGULAR_ORDER)
+    return 0;
+  if (c.engine > XGPU_ENGINE_TENSOR) return 0;
+  if (c.engine == XGPU_ENGINE_TENSOR && c.compute_type != XGPU_INT8) return 0;
+  if (c.input_format > XGPU_INPUT_BLOCK32) return 0;
+  // channel range: [channel_offset, channel_offset + nfrequency) of the band
+  const unsigned band = c.input_nfrequency ? c.input_nfrequency : c.nfrequency;
+  if (!c.input_nfrequency && c.channel_offset) return 0;
+  if (band > 65535 || c.channel_offset > band || band - c.channel_offset < c.nfrequency) return 0;
+  // input bytes of one call must fit the 32-bit sample index space of the engines
+  const double bytes = 4.0 * c.nstation * band * (double)c.ntime;
+  if (bytes > 1.0e12) return 0;
+  return 1;
+}
+
 Sizes make_sizes(const XGPUConfig &c) {
   Sizes s;
   s.n = (int)c.nstation;
@@ -545,6 +584,26 @@ Sizes make_sizes(const XGPUConfig &c) {
                      ? (long long)s.f * (s.n / 2 + 1) * (s.n / 4) * kNpol * kNpol * 4
                      : s.tri_length;
   s.state_elems = 2 * s.tri_length;
+  s.fband = c.input_nfrequency ? (int)c.input_nfrequency : s.f;
+  s.fin = s.fband;
+  s.fin0 = (int)c.channel_offset;
+  // One row of the input holds every channel of one sample (of four samples
+  // in xGPU's DP4A swizzle), each channel's bytes contiguous.
+  switch (c.input_format) {
+    case XGPU_INPUT_PACKED4:
+      s.chan_bytes = (long long)s.n * kNpol;
+      s.rows = s.t;
+      break;
+    case XGPU_INPUT_DP4A_SWIZZLED:
+      s.chan_bytes = (long long)s.n * kNpol * 2 * 4;
+      s.rows = s.t / 4;
+      break;
+    default:   // int8 and xGPU's COMPLEX_BLOCK_SIZE=32 (blocks of 16 stations of one channel)
+      s.chan_bytes = (long long)s.n * kNpol * 2;
+      s.rows = s.t;
+      break;
+  }
+  s.band_bytes = s.rows * s.fband * s.chan_bytes;
   return s;
 }
 
@@ -584,7 +643,7 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
   XGPUConfig cfg = *cfg_in;
   if (cfg.engine == XGPU_ENGINE_DEFAULT)
     cfg.engine = cfg.compute_type == XGPU_INT8 ? XGPU_ENGINE_TENSOR : XGPU_ENGINE_PLAIN;
-  if (!validate(cfg)) return XGPU_INVALID_ARGUMENT;
+  if (!validate_config(cfg)) return XGPU_INVALID_ARGUMENT;
 
   Internal *in = new (std::nothrow) Internal();
   if (!in) return XGPU_OUT_OF_MEMORY;
@@ -594,6 +653,7 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
   in->register_host_matrix = !(device_flags & XGPU_DONT_REGISTER_MATRIX);
   in->cfg = cfg;
   in->sz = make_sizes(cfg);
+  in->szc = compact_sizes(in->sz);
   in->int_state = cfg.compute_type == XGPU_INT8;
   // CTA-pair 256x256 tiles pay off once a channel has several of them; the
   // autotuner (xgpuTune) revisits the choice per shape.
@@ -636,7 +696,8 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
       cudaMallocHost(&in->h_err, sizeof(int)) != cudaSuccess ||
       (cfg.input_format != XGPU_INPUT_INT8 &&
        (cudaMalloc(&in->d_conv[0], (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess ||
-        cudaMalloc(&in->d_conv[1], (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess))) {
+        cudaMalloc(&in->d_conv[1], (size_t)(2 * s.vec_length + 255) / 256 * 256) != cudaSuccess ||
+        (s.fband != s.f && cudaMalloc(&in->d_slice, in_bytes) != cudaSuccess)))) {
     cudaGetLastError();
     return fail(XGPU_OUT_OF_MEMORY);
   }
@@ -718,7 +779,7 @@ int xgpuSetHostInputBuffer(XGPUContext *context) {
       in->unregister_array_h = (ComplexInput *)reg;
     }
   } else {
-    const size_t bytes = (size_t)in->sz.input_bytes;
+    const size_t bytes = (size_t)in->sz.band_bytes;
     // array_len counts ComplexInput elements (2 bytes); packed input needs half.
     context->array_len = (bytes + sizeof(ComplexInput) - 1) / sizeof(ComplexInput);
     XGPU_CHECK(cudaMallocHost((void **)&context->array_h, context->array_len * sizeof(ComplexInput)));
@@ -790,7 +851,7 @@ int xgpuCudaXengine(XGPUContext *context, int syncOp) {
   if (!in->array_h_set || !in->matrix_h_set) return XGPU_HOST_BUFFER_NOT_SET;
   if (syncOp < SYNCOP_NONE || syncOp > SYNCOP_SYNC_COMPUTE) return XGPU_INVALID_ARGUMENT;
   if (!context->array_h) return XGPU_HOST_BUFFER_NOT_SET;
-  const size_t need = (size_t)((in->sz.input_bytes + 1) / 2);  // in ComplexInput units
+  const size_t need = (size_t)((in->sz.band_bytes + 1) / 2);  // in ComplexInput units
   if (context->array_len && context->input_offset + need > context->array_len)
     return XGPU_INVALID_ARGUMENT;
   XGPU_CHECK(cudaSetDevice(in->device));
@@ -803,10 +864,20 @@ int xgpuCudaXengine(XGPUContext *context, int syncOp) {
   }
   // The buffer is free once the engine launch that last read it has finished.
   XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
-  XGPU_CHECK(cudaMemcpyAsync(in->d_in[b], context->array_h + context->input_offset,
-                             (size_t)in->sz.input_bytes, cudaMemcpyHostToDevice, in->s_copy));
+  const Sizes &s = in->sz;
+  if (s.fband == s.f) {
+    XGPU_CHECK(cudaMemcpyAsync(in->d_in[b], context->array_h + context->input_offset,
+                               (size_t)s.input_bytes, cudaMemcpyHostToDevice, in->s_copy));
+  } else {
+    // this context's channels of every row of the band
+    XGPU_CHECK(cudaMemcpy2DAsync(in->d_in[b], (size_t)(s.f * s.chan_bytes),
+                                 (const char *)(context->array_h + context->input_offset) +
+                                     s.fin0 * s.chan_bytes,
+                                 (size_t)(s.fband * s.chan_bytes), (size_t)(s.f * s.chan_bytes),
+                                 (size_t)s.rows, cudaMemcpyHostToDevice, in->s_copy));
+  }
   XGPU_CHECK(cudaEventRecord(in->copy_done[b], in->s_copy));
-  int r = run_engine(in, in->d_in[b], in->copy_done[b]);
+  int r = run_engine(in, in->d_in[b], in->copy_done[b], true);
   if (r != XGPU_OK) return r;
   XGPU_CHECK(cudaEventRecord(in->comp_done[b], in->s_comp));
   in->adding_tail = false;
@@ -819,7 +890,7 @@ int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int sy
   if (!device_input || ((uintptr_t)device_input & 15) != 0) return XGPU_INVALID_ARGUMENT;
   if (syncOp < SYNCOP_NONE || syncOp > SYNCOP_SYNC_COMPUTE) return XGPU_INVALID_ARGUMENT;
   XGPU_CHECK(cudaSetDevice(in->device));
-  int r = run_engine(in, device_input, nullptr);
+  int r = run_engine(in, device_input, nullptr, false);
   if (r != XGPU_OK) return r;
   return finish_call(context, in, syncOp);
 }
@@ -885,7 +956,7 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
   if (!in->int_state || in->cfg.engine != XGPU_ENGINE_TENSOR) return XGPU_OK;  // nothing to tune
   XGPU_CHECK(cudaSetDevice(in->device));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
-  const Sizes &s = in->sz;
+  const Sizes &s = in->szc;   // the tuning input is a compact buffer
   // Synthetic int8 input where the engine reads it -- the first input buffer
   // of an int8 context (its contents are replaced by the next call anyway),
   // the first conversion buffer of the other formats (the input buffers of a
