@@ -212,6 +212,63 @@ def e2e_ms(xg, oracle, n, f, t, steps, warmup, device):
     return ms, h2d, d2h, ok
 
 
+def e2e_streaming(xg, oracle, n, f, t, calls, reps, device):
+    """The reference driver's own call pattern (cuda_correlator.c:196-230,
+    defaults :46-47): an integration of `calls` xgpuCudaXengine calls over host
+    buffers, SYNCOP_SYNC_TRANSFER on all but the last, SYNCOP_DUMP on the last
+    (copy of each call's input under the previous call's correlation, one dump
+    per integration).  Host wall clock over `reps` integrations."""
+    c = xg.Correlator(n, f, t, engine="tensor", output="int32", order="tri", device=device)
+    x = oracle.gaussian_input(n, f, t, seed=1, sigma=SIGMA)
+    c.set_input(x)
+
+    def integration():
+        c.clear()
+        for q in range(calls):
+            c.run(xg.SYNCOP_DUMP if q == calls - 1 else xg.SYNCOP_SYNC_TRANSFER)
+    for _ in range(2):
+        integration()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        integration()
+    ms = (time.perf_counter() - t0) * 1e3 / reps
+    got = c.output_view()[: c.info.matLength * 2]
+    ok = bool((got == (calls * oracle.xengine_i64(x, n, f, t)).astype("int32")).all())
+    h2d = calls * int(c.info.vecLength) * 2
+    d2h = int(c.info.matLength) * 8
+    c.close()
+    return {"calls_per_integration": calls, "integrations": reps,
+            "ms_per_call": ms / calls, "tops": calls * ops(n, f, t) / (ms * 1e-3) / 1e12,
+            "h2d_bytes_per_integration": h2d, "d2h_bytes_per_integration": d2h,
+            "host_link_gbs": (h2d + d2h) / (ms * 1e-3) / 1e9, "bit_exact_vs_oracle": ok,
+            "syncops": "SYNCOP_SYNC_TRANSFER x (calls-1), SYNCOP_DUMP"}
+
+
+def fp32_engine_long(xg, oracle, device, n=32, f=2, t=32768, sigma=40.0):
+    """The plain FP32 engine where float sums round (autos ~1e8 > 2^24): its
+    relative error against the reference's float arithmetic (the oracle's
+    restatement of omp_xengine.c:24-28; the stated tolerance is 1e-6) and, for
+    context, both against the exact int64 sums."""
+    import numpy as np
+    x = oracle.gaussian_input(n, f, t, seed=5, sigma=sigma)
+    with xg.Correlator(n, f, t, engine="plain", compute="fp32", output="float32",
+                       device=device) as c:
+        c.set_input(x)
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2].astype(np.float64)
+    ref = oracle.xengine_f32(x, n, f, t).astype(np.float64)
+    exact = oracle.xengine_i64(x, n, f, t).astype(np.float64)
+    nz = ref != 0
+    nze = exact != 0
+    return {"nstation": n, "nfrequency": f, "ntime": t, "sigma": sigma,
+            "max_abs_sum": float(np.abs(exact).max()),
+            "max_rel_err_vs_reference_float": float((np.abs(got - ref)[nz] / np.abs(ref[nz])).max()),
+            "tolerance": 1e-6,
+            "max_rel_err_vs_exact": float((np.abs(got - exact)[nze] / np.abs(exact[nze])).max()),
+            "reference_float_max_rel_err_vs_exact":
+                float((np.abs(ref - exact)[nze] / np.abs(exact[nze])).max())}
+
+
 def float_output_error(xg, oracle, n, f, t, sigma, device):
     """Float32-output mode against the FP64 host oracle: one call, dumped as
     float32 (the exact int64 sums are rounded once, at dump).  Returns the max
@@ -249,7 +306,9 @@ def uneven_subarray_shapes(seed=3, k=96):
 
 def bench_uneven_batch(xg, torch, steps):
     """One persistent launch over 96 uneven subarrays (autotuned, CUDA graph)
-    vs the same jobs run one by one on the tensor-core and plain engines."""
+    vs the same jobs run one by one on the tensor-core and plain engines; every
+    job's batched sums are compared with the plain engine's."""
+    import numpy as np
     shapes = uneven_subarray_shapes()
     dev = torch.cuda.current_device()
     stream = torch.cuda.Stream()
@@ -278,7 +337,12 @@ def bench_uneven_batch(xg, torch, steps):
         ms = e0.elapsed_time(e1) / k
     out["batched_ms"] = ms
     out["batched_tops"] = total_ops / (ms * 1e-3) / 1e12
-    batched = [s.clone() for s in states[:6]]
+    # The batch's buffers now hold its last run; the job-by-job contexts below
+    # have buffers of their own, so every job's batched result is compared
+    # with the plain engine's, bit for bit.
+    out["jobs_compared_vs_plain"] = 0
+    out["bit_exact_vs_plain"] = True
+    out["max_nstation_compared"] = 0
     # job by job on each engine (per-call device time summed)
     for engine in ("tensor", "plain"):
         tot = 0.0
@@ -294,10 +358,11 @@ def bench_uneven_batch(xg, torch, steps):
                 a1.record(st)
                 a1.synchronize()
                 tot += a0.elapsed_time(a1)
-                if engine == "plain" and q < len(batched):
-                    out.setdefault("bit_exact_vs_plain", True)
-                    got = torch.from_numpy(c.dump_int64()).cuda()
-                    out["bit_exact_vs_plain"] &= bool(torch.equal(got, batched[q]))
+                if engine == "plain":
+                    same = bool(np.array_equal(c.dump_int64(), states[q].cpu().numpy()))
+                    out["bit_exact_vs_plain"] &= same
+                    out["jobs_compared_vs_plain"] += 1
+                    out["max_nstation_compared"] = max(out["max_nstation_compared"], n)
         out[f"{engine}_job_by_job_ms"] = tot
         out[f"{engine}_job_by_job_tops"] = total_ops / (tot * 1e-3) / 1e12
     out["batched_over_plain_job_by_job"] = out["plain_job_by_job_ms"] / out["batched_ms"]
@@ -327,11 +392,49 @@ def served_requests(seconds, seed=4, rate_jobs=200.0):
 SAMPLE_RATE = 1.0e5   # per-channel complex samples/s of the served stream
 
 
+def request_ops(r):
+    return ops(r["nstation"], r["nfrequency"], r["ntime"]) * r["nblocks"]
+
+
+def served_check_sample(reqs, k=12, max_ops=3e11, seed=5):
+    """Indices of served requests whose dumps the bench checks against the
+    oracle: a seeded draw of k requests among those the oracle integrates in
+    a few seconds on the host (at most max_ops), plus the cheapest request
+    with N > 512."""
+    import numpy as np
+    cheap = [q for q, r in enumerate(reqs) if request_ops(r) <= max_ops]
+    rng = np.random.default_rng(seed)
+    pick = set(int(q) for q in rng.choice(cheap, size=min(k, len(cheap)), replace=False))
+    big = [q for q, r in enumerate(reqs) if r["nstation"] > 512]
+    if big:
+        pick.add(min(big, key=lambda q: request_ops(reqs[q])))
+    return sorted(pick)
+
+
+def served_expected(oracle, r):
+    """Final int32 triangular dump of a served request, from the oracle."""
+    import numpy as np
+    n, f, t = r["nstation"], r["nfrequency"], r["ntime"]
+    acc = np.zeros(f * n * (n + 1) // 2 * 8, dtype=np.int64)
+    for b in range(r["nblocks"]):
+        x = oracle.serve_block_input(n, f, t, r["seed"], r["sigma"], b)
+        oracle.xengine_i64(x, n, f, t, acc=acc)
+    return acc.astype(np.int32)
+
+
 def bench_served_stream(xg, seconds, plain_seconds, device):
+    import numpy as np
+    import oracle
     reqs = served_requests(seconds)
-    st, _ = xg.serve(reqs, SAMPLE_RATE, 120 << 30, host_budget_bytes=24 << 30, device=device)
+    check = served_check_sample(reqs)
+    st, res = xg.serve(reqs, SAMPLE_RATE, 120 << 30, host_budget_bytes=24 << 30, device=device,
+                       collect=check)
+    exact = [bool(np.array_equal(res[q], served_expected(oracle, reqs[q]))) for q in check]
     out = {"arrival_rate_per_s": 200.0, "seconds": seconds, "sample_rate_hz": SAMPLE_RATE,
-           "requests": len(reqs), "served": st}
+           "requests": len(reqs), "served": st,
+           "served_bit_exact_sampled": all(exact), "sampled_requests": len(check),
+           "sampled_max_nstation": max(reqs[q]["nstation"] for q in check),
+           "sampled_ops": sum(request_ops(reqs[q]) for q in check)}
     if plain_seconds > 0:
         reqs_p = served_requests(plain_seconds)
         sp, _ = xg.serve(reqs_p, SAMPLE_RATE, 120 << 30, mode=xg.XGPU_SERVE_PLAIN_SERIAL,
@@ -341,12 +444,27 @@ def bench_served_stream(xg, seconds, plain_seconds, device):
     return out
 
 
-def bench_large_array(xg, torch, device, blocks=64):
+def channel_input(oracle, kind, seed, sigma, n, f_total, t, f):
+    """Channel f's samples ([t][s][p][c] int8) of a seeded device-generated
+    block [t][f_total][s][p] (kind 0: int8 {re,im}; kind 1: packed 4+4-bit),
+    regenerated on the host: the generator's byte k depends only on (seed, k)."""
+    import numpy as np
+    width = n * (4 if kind == 0 else 2)
+    rows = [oracle.generate(width, kind, seed, sigma, offset=(q * f_total + f) * width)
+            for q in range(t)]
+    x = np.concatenate(rows)
+    return x if kind == 0 else oracle.unpack4(x)
+
+
+def bench_large_array(xg, torch, device, blocks=64, check_channels=(0, F3 - 1)):
     """The large-array configuration: N=512, F=256, T=8192 per block, 64 blocks
     integrated before one dump, with packed 4+4-bit input expanded on the device
     (uniform [-7,7]) and an int8 variant (sigma 40).  Two distinct input blocks
-    alternate (4.3 / 2.1 GB each, far above L2); exactness is checked by
-    linearity: 64 blocks alternating A, B must equal 32 x (A + B)."""
+    alternate (4.3 / 2.1 GB each, far above L2).  Exactness: the first block's
+    sums on two channels equal the oracle's (int64, omp_xengine.c:45-89), and
+    64 blocks alternating A, B equal 32 x (A + B) (linearity, every channel)."""
+    import numpy as np
+    import oracle
     out = {"nstation": N3, "nfrequency": F3, "ntime": T3, "blocks": blocks}
     for fmt, kind, sig in (("packed4", 1, 0.0), ("int8", 0, 40.0)):
         # The context's own streams (packed input is expanded on a side stream
@@ -361,9 +479,18 @@ def bench_large_array(xg, torch, device, blocks=64):
             x = torch.empty(nbytes, dtype=torch.int8, device="cuda")
             xg.generate_device(x.data_ptr(), nbytes, kind, 9000 + q, sig or 16.0, device)
             bufs.append(x)
-        # A + B once, for the linearity check
+        # A alone: sampled channels against the oracle; then A + B, for the
+        # linearity check
         c.clear()
-        c.run_device(bufs[0].data_ptr(), xg.SYNCOP_NONE)
+        c.run_device(bufs[0].data_ptr(), xg.SYNCOP_SYNC_COMPUTE)
+        a_sums = c.dump_int64()
+        nb8 = N3 * (N3 + 1) // 2 * 8
+        channels_exact = True
+        for f in check_channels:
+            x = channel_input(oracle, kind, 9000, sig or 16.0, N3, F3, T3, f)
+            want = oracle.xengine_i64(x, N3, 1, T3)
+            channels_exact &= bool(np.array_equal(a_sums[f * nb8:(f + 1) * nb8], want))
+        del a_sums
         c.run_device(bufs[1].data_ptr(), xg.SYNCOP_SYNC_COMPUTE)
         ab = torch.from_numpy(c.dump_int64())
         c.clear()
@@ -378,7 +505,9 @@ def bench_large_array(xg, torch, device, blocks=64):
         out[fmt] = {"ms_total": ms, "ms_per_block": ms / blocks, "tops": o / (ms * 1e-3) / 1e12,
                     "max_abs_visibility": int(full.abs().max()),
                     "exceeds_int32": bool(full.abs().max() > 2**31 - 1),
-                    "linearity_exact": bool(torch.equal(full, (blocks // 2) * ab))}
+                    "linearity_exact": bool(torch.equal(full, (blocks // 2) * ab)),
+                    "oracle_channels_exact": channels_exact,
+                    "oracle_channels": list(check_channels)}
         c.close()
         del bufs
         torch.cuda.empty_cache()
@@ -491,10 +620,11 @@ def main():
                          "profiler's serialised launches mislead the autotuner)")
     ap.add_argument("--no-detail", action="store_true",
                     help="skip the plain, N=512, batched and served legs")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
-                    help="seconds of Poisson arrivals for the served stream (60 = full config)")
-    ap.add_argument("--plain-serve-seconds", type=float, default=0.5,
-                    help="seconds of arrivals for the one-at-a-time plain baseline")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="seconds of Poisson arrivals for the served stream")
+    ap.add_argument("--plain-serve-seconds", type=float, default=2.0,
+                    help="seconds of arrivals for the one-at-a-time plain baseline (it falls "
+                         "behind the arrivals, so its latency grows with this)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
@@ -530,12 +660,19 @@ def main():
             pk = xg.core_peak(kind, local) / 1e12
             detail[f"core_{kind}_peak_tops_measured"] = pk
             detail[f"plain_{kind}_n256_frac_of_core_peak"] = detail[f"plain_{kind}_n256_tops"] / pk
+        # The FP32 engine adds each sample's exact product pair with one
+        # rounding, as xGPU's float engine does: 6 FP32 instructions (FMUL,
+        # FFMA, FADD per component) per complex MAC of 8 operations, where the
+        # measured rate counts 4 FMAs.  Its instruction ceiling is 4/6 of it.
+        detail["plain_fp32_n256_frac_of_instruction_ceiling"] = (
+            detail["plain_fp32_n256_tops"] / (detail["core_fp32_peak_tops_measured"] * 4 / 6))
         if rank == 0:
             # the default shape itself (every sum below 2^24: exact) and a long
             # integration whose sums pass 2^24
             detail["float32_output_n256_f10_t1024"] = float_output_error(xg, oracle, N, F, T, SIGMA, local)
             detail["float32_output_long"] = float_output_error(xg, oracle, 64, 10, 32768, 40.0,
                                                                local)
+            detail["fp32_engine_vs_reference_float"] = fp32_engine_long(xg, oracle, local)
         k3 = max(3, min(args.steps, 10))
         ms3, _ = device_engine_ms(xg, torch, "tensor", "int8", N3, F3, T3, k3, 2, world,
                                   sigma=40.0, min_rotate_bytes=0, max_bufs=1)
@@ -562,6 +699,9 @@ def main():
                  # group by channel group (the two directions overlap): the
                  # host link sets the pace
                  "host_link_gbs": (h2d + d2h) / (ms_e * 1e-3) / 1e9}
+        if not args.no_detail and world == 1:
+            detail["e2e_streaming"] = e2e_streaming(xg, oracle, N, F, T, 8, max(3, min(args.steps, 20)),
+                                                    local)
     clk = clocks.stop()
     peak8 = int8_peak_tops(torch) if rank == 0 else None
     if rank != 0:
@@ -610,14 +750,18 @@ def main():
         "vs_baseline": None, "dtype": "int8",
         "data": "synthetic: seeded Gaussian int8 samples, sigma 16 (counter-based generator)",
         "config": {"workload": f"xGPU default shape NSTATION={N} NPOL=2 NFREQUENCY={F} NTIME={T}: "
-                               "one xgpuCudaXengine call per step, tcgen05 int8 engine, int64 "
-                               "integration buffer",
+                               "one xgpuCudaXengineDevice call per step on input resident in "
+                               "HBM (SYNCOP_NONE, accumulating), tcgen05 int8 engine, int64 "
+                               "integration buffer; host buffers and copies: see e2e",
                    "nstation": N, "npol": 2, "nfrequency": F, "ntime": T,
                    "parallelism": f"channel-sharded replicas x{world} (no collective)",
                    "l2": f"input rotates over {rot_bytes / 2**20:.0f} MiB of buffers (> 126 MiB L2)",
                    "tuning": TUNING.get(("tensor", N, F, T)),
                    "launches": "programmatic (PDL): each accumulating call may start while the "
-                               "previous call's launch finishes; ms_per_step is the spacing"},
+                               "previous call's launch finishes; ms_per_step is the spacing",
+                   "timing": "CUDA events on the context's stream around the K calls; the "
+                             "time includes filling and draining the chain of overlapping "
+                             "launches (about 35 us per run), so short runs read lower"},
         "e2e": e2e_v, "gpu_launches": args.steps, "roofline": roof,
         "cpu_baseline": cpu_baseline(), "clocks": clk, "detail": detail,
     }

@@ -1,9 +1,10 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
-Run in a container that has the reference sources (the _ref/ libraries are
-built from them by ``make -C oracle``)::
+Run where the reference sources are (the _ref/ libraries are built from them
+by ``make -C oracle``), with XGPU_REF_SRC naming the reference's src/
+directory unless it is checked out beside this repository::
 
-    python tests/golden/make_golden.py
+    XGPU_REF_SRC=<xGPU>/src python tests/golden/make_golden.py
 
 Every array stored here is an output of the reference's own CPU code
 (xGPU ``src/omp_xengine.c`` and ``src/cpu_util.c`` compiled per shape), on
@@ -24,7 +25,15 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 import oracle  # noqa: E402
 
 
-REF_SRC = "/root/reference/src"
+def reference_src():
+    """The reference's src/ directory: $XGPU_REF_SRC, else a checkout beside
+    this repository (../reference/src)."""
+    path = os.environ.get("XGPU_REF_SRC") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "..", "reference", "src")
+    if not os.path.exists(os.path.join(path, "omp_xengine.c")):
+        sys.exit("make_golden.py: the reference's src/ directory was not found; "
+                 "set XGPU_REF_SRC to it")
+    return os.path.abspath(path)
 
 
 def abi_facts(include_dir, flags):
@@ -44,6 +53,8 @@ def sha(a):
 
 
 def main():
+    ref_src = reference_src()
+    os.environ["XGPU_REF_SRC"] = ref_src
     oracle.build()
     if not oracle.ref_available("s16", "fp32_rt"):
         raise SystemExit("reference libraries missing: run make -C oracle where the reference exists")
@@ -101,7 +112,7 @@ def main():
     # ABI facts of the reference header, plain and with DP4A.
     meta["abi"] = {}
     for tag, flags in [("plain", []), ("dp4a", ["-DDP4A"])]:
-        meta["abi"][tag] = abi_facts(REF_SRC, flags)
+        meta["abi"][tag] = abi_facts(ref_src, flags)
 
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **arrays)
     with open(os.path.join(HERE, "golden.json"), "w") as fh:

@@ -44,3 +44,27 @@ def test_ops_formula_is_the_reference_flop_count():
     # 16 F T N(N+1): 8 operations per complex multiply-add over N(N+1)/2
     # baselines and 4 polarisation products (kernel.cuh:419)
     assert bench.ops(256, 10, 1024) == 16 * 10 * 1024 * 256 * 257
+
+
+def test_served_check_sample_is_seeded_and_covers_a_large_array():
+    reqs = bench.served_requests(60.0)
+    pick = bench.served_check_sample(reqs)
+    assert pick == bench.served_check_sample(reqs)
+    assert len(pick) >= 12
+    assert any(reqs[q]["nstation"] > 512 for q in pick)
+    small = [q for q in pick if reqs[q]["nstation"] <= 512]
+    assert all(bench.request_ops(reqs[q]) <= 3e11 for q in small)
+
+
+def test_channel_input_is_the_channel_of_the_generated_block(oracle_mod):
+    """The large-array leg regenerates one channel of a device-generated block
+    on the host; it must be that channel's slice of the whole block."""
+    n, f_total, t = 32, 5, 64
+    for kind, width in ((0, 4), (1, 2)):
+        full = oracle_mod.generate(t * f_total * n * width, kind, 9000, 40.0)
+        for f in (0, f_total - 1):
+            want = np.ascontiguousarray(full.reshape(t, f_total, n * width)[:, f, :]).reshape(-1)
+            if kind == 1:
+                want = oracle_mod.unpack4(want)
+            got = bench.channel_input(oracle_mod, kind, 9000, 40.0, n, f_total, t, f)
+            assert np.array_equal(got, want)

@@ -119,7 +119,45 @@ def test_range_in_register_tile_order(xg, oracle_mod):
         assert view.size == x.size
         c.set_input(x)
         c.run(xg.SYNCOP_DUMP)
-        got = c.output_view()[: c.info.matLength * 2]
+        got = c.output_view()[: c.info.matLength * 2].copy()   # the view dies with the context
     sub = np.ascontiguousarray(x.reshape(t, f, n * 4)[:, 2:7, :]).reshape(-1)
     exact = oracle_mod.xengine_i64(sub, n, 5, t)
     assert np.array_equal(got, oracle_mod.tri_to_order(exact.astype(np.int32), n, 5, 3000))
+
+
+def test_shared_pinned_band_and_output_without_registration(xg, oracle_mod):
+    """The multi-GPU calling pattern of the integration guide, on one GPU: one
+    caller-pinned band and one caller-pinned triangular output shared by
+    three contexts created with XGPU_DONT_REGISTER; each context dumps its
+    range into its part of the output (ranges share pages at their ends), and
+    the whole output is the band's matrix."""
+    import ctypes
+    import torch
+    n, f, t = 128, 9, 512
+    nb = n * (n + 1) // 2
+    ranges = [(0, 4), (4, 5), (5, 9)]
+    x = oracle_mod.gaussian_input(n, f, t, seed=71, sigma=18.0)
+    band = torch.from_numpy(x).pin_memory()
+    out = torch.zeros(f * nb * 8, dtype=torch.int32).pin_memory()
+    ctxs = []
+    try:
+        for f0, f1 in ranges:
+            c = ranged(xg, n, f0, f1, f, t, engine="tensor", order="tri",
+                       flags=xg.XGPU_DONT_REGISTER)
+            ctxs.append(c)
+            c.ctx.array_h = band.data_ptr()
+            c.ctx.array_len = t * f * n * 2
+            c.ctx.matrix_h = out.data_ptr() + f0 * nb * 4 * 8
+            c.ctx.matrix_len = (f1 - f0) * nb * 4
+            xg.check("xgpuSetHostInputBuffer", xg.lib().xgpuSetHostInputBuffer(ctypes.byref(c.ctx)))
+            xg.check("xgpuSetHostOutputBuffer",
+                     xg.lib().xgpuSetHostOutputBuffer(ctypes.byref(c.ctx)))
+        for c in ctxs:
+            c.run(xg.SYNCOP_NONE)
+        for c in ctxs:
+            c.run(xg.SYNCOP_DUMP)           # a second integration step, dumped
+    finally:
+        for c in ctxs:
+            c.close()
+    want = (2 * oracle_mod.xengine_i64(x, n, f, t)).astype(np.int32)
+    assert np.array_equal(out.numpy(), want)

@@ -400,7 +400,9 @@ def serve(requests, sample_rate_hz, device_budget_bytes, mode=XGPU_SERVE_BATCHED
           host_budget_bytes=0, collect=False):
     """Run xgpuServeRun on a list of request dicts (nstation, nfrequency, ntime,
     nblocks, dump_every, seed, sigma, arrival_s).  Returns (stats dict, results)
-    where results are the final int32 triangular dumps when collect=True."""
+    where results are the final int32 triangular dumps when collect=True, or,
+    when collect is a collection of request indices, a dict index -> dump of
+    those requests only."""
     arr = (XGPUServeJob * len(requests))()
     for a, r in zip(arr, requests):
         a.nstation, a.nfrequency, a.ntime = r["nstation"], r["nfrequency"], r["ntime"]
@@ -410,11 +412,19 @@ def serve(requests, sample_rate_hz, device_budget_bytes, mode=XGPU_SERVE_BATCHED
     st = XGPUServeStats()
     res_ptrs = None
     results = None
-    if collect:
-        results = [np.zeros(r["nfrequency"] * r["nstation"] * (r["nstation"] + 1) // 2 * 8,
-                            dtype=np.int32) for r in requests]
+
+    def words(r):
+        return np.zeros(r["nfrequency"] * r["nstation"] * (r["nstation"] + 1) // 2 * 8,
+                        dtype=np.int32)
+    if collect is True:
+        results = [words(r) for r in requests]
         res_ptrs = (ctypes.POINTER(ctypes.c_int) * len(requests))(
             *[x.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) for x in results])
+    elif collect:
+        results = {q: words(requests[q]) for q in sorted(set(collect))}
+        res_ptrs = (ctypes.POINTER(ctypes.c_int) * len(requests))()
+        for q, x in results.items():
+            res_ptrs[q] = x.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
     check("xgpuServeRun", lib().xgpuServeRun(arr, len(requests), ctypes.byref(opt),
                                              ctypes.byref(st), res_ptrs))
     stats = {name: getattr(st, name) for name, _ in XGPUServeStats._fields_}
