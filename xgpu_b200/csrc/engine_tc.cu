@@ -60,7 +60,7 @@ constexpr int kStageBytes = 2 * kBoxBytes;
 // One station row of the staging tile; 16 bytes of padding put the 8 rows a
 // warp writes on distinct 16-byte bank groups, and five 32 KB stages still
 // fit in 227 KB.
-constexpr int kRowPitch = kPitchPairs;
+constexpr int kRowPitch = kStations * 64 + 16;
 constexpr int kStateBytes = kStations * kRowPitch;
 constexpr int kBarrierBytes = 512;    // barriers, work-item ring, TMEM slot
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
@@ -89,7 +89,7 @@ struct Item {
   int u;               // work item index (>= total: no more work)
   int f, tr, tc;
   int step0, nsteps;   // pipeline stages of this item (its time split)
-  int n, store, t0, words;   // words: Job::words
+  int n, store, t0, pad;
   long long nbaseline;
   int64_t *state;
   const CUtensorMap *map;
@@ -114,7 +114,7 @@ __device__ __forceinline__ Item decode_job(const Job &j, int u) {
   it.n = j.n;
   it.store = j.store;
   it.t0 = j.t0;
-  it.words = j.words;
+  it.pad = 0;
   it.nbaseline = j.nbaseline;
   it.state = j.state;
   it.map = &j.map;
@@ -136,21 +136,19 @@ __device__ __forceinline__ Item decode_item(const Params &p, int u) {
 }
 
 // Bytes of station row il (0..31) of the item's tile inside the integration
-// buffer: baselines (i, j) with j in the tile's column block, j <= i, j < n;
-// 64 bytes per baseline (int64 pairs), 32 in the word format.
+// buffer: baselines (i, j) with j in the tile's column block, j <= i, j < n.
 __device__ __forceinline__ int row_bytes(const Item &t, int il) {
   const int i = t.tr * kStations + il;
   if (i >= t.n) return 0;
   int cnt = t.n - t.tc * kStations;
   if (cnt > kStations) cnt = kStations;
   if (t.tr == t.tc && il + 1 < cnt) cnt = il + 1;
-  return cnt * (t.words ? 32 : 64);
+  return cnt * 64;
 }
 
 __device__ __forceinline__ int64_t *row_ptr(const Item &t, int il) {
   const long long i = (long long)t.tr * kStations + il;
-  return t.state + ((long long)t.f * t.nbaseline + i * (i + 1) / 2 + (long long)t.tc * kStations) *
-                       (t.words ? 4 : 8);
+  return t.state + ((long long)t.f * t.nbaseline + i * (i + 1) / 2 + (long long)t.tc * kStations) * 8;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_constant__ Params p) {
@@ -360,8 +358,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       }
       __syncwarp();
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint8_t *srow = t.words ? sstate + il * kPitchWords + (p1 * 2 + c) * 8
-                              : sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+      uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
       int jmax = t.n - t.tc * kStations;
       if (jmax > kStations) jmax = kStations;
       if (t.tr == t.tc && il + 1 < jmax) jmax = il + 1;
@@ -386,10 +383,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
           const long long re = c ? (long long)ra + v3 : (long long)v0 + rb;
           const long long im = c ? (long long)v2 - rb : (long long)ra - v1;
           const int jl = q * 8 + jj;
-          if (jl < jmax) {
-            if (t.words) *(long long *)(srow + jl * 32) = visibility_word(re, im);
-            else *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
-          }
+          if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
         }
       }
       // Staging rows complete: hand them to the bulk-copy engine.
@@ -398,7 +392,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       if (copier) {
         const int nb = row_bytes(t, lane);
         if (nb) {
-          const uint32_t src = smem_u32(sstate + lane * (t.words ? kPitchWords : kRowPitch));
+          const uint32_t src = smem_u32(sstate + lane * kRowPitch);
           if (t.store) bulk_store(row_ptr(t, lane), src, nb);
           else bulk_reduce_add(row_ptr(t, lane), src, nb);
         }
@@ -538,7 +532,6 @@ int tc_fill_job(Job *job, const void *dev_in, const Sizes &s, int t0, int tcount
   job->items = (int)(s.f * npairs * ksplit);
   job->item_begin = item_begin;
   job->store = (store && ksplit == 1) ? 1 : 0;
-  job->words = 0;
   return 0;
 }
 
@@ -550,14 +543,12 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
-                            const TcTuning &tune, int overlap, int f0, int fcount, int packed,
-                            int words) {
+                            const TcTuning &tune, int overlap, int f0, int fcount, int packed) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
-  if (words && tcount > kWordSamples) return cudaErrorInvalidValue;
   if (tune.wide)
     return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap, f0, fcount,
-                      packed, words);
+                      packed);
   if (packed) return cudaErrorInvalidValue;   // only the CTA-pair kernel expands packed input
   const int sms = current_device_sms();
   if (!sms) return cudaErrorInvalidDevice;
@@ -579,14 +570,12 @@ cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int 
   // Split items of one tile all add into the buffer: a zero buffer must be
   // cleared first (its channel range) when it would otherwise be stored into.
   if (overwrite && ksplit > 1) {
-    // int64 values per channel: (re, im) pairs, or one word per visibility
-    const size_t per_channel = (size_t)s.state_elems / s.f / (words ? 2 : 1);
+    const size_t per_channel = (size_t)s.state_elems / s.f;   // int64 words
     cudaError_t e = cudaMemsetAsync(state + (size_t)f0 * per_channel, 0,
                                     (size_t)fcount * per_channel * 8, st);
     if (e != cudaSuccess) return e;
   }
   j.state = state;
-  j.words = words ? 1 : 0;
   j.nbaseline = s.nbaseline;
   j.n = s.n;
   j.f = fcount;

@@ -54,7 +54,7 @@ constexpr int kBoxBytes = kHalf * kKt;      // 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;  // A rows + B half
 // 16 bytes of padding per 2 KB row: the 8 rows a warp writes fall on distinct
 // 16-byte bank groups, and five 32 KB stages still fit in 227 KB.
-constexpr int kRowPitch = kPitchPairs;
+constexpr int kRowPitch = kStations * 64 + 16;
 constexpr int kStateBytes = kStations * kRowPitch;   // one 32x32-station block
 constexpr int kBarrierBytes = 512;    // barriers, work-item ring, TMEM slot
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
@@ -94,7 +94,7 @@ struct Item {
   int u;               // >= total: no more work
   int f, R, C;         // channel and 256x256 tile (R >= C)
   int step0, nsteps;
-  int n, store, t0, words;   // words: Job::words
+  int n, store, t0, pad;
   long long nbaseline;
   int64_t *state;
   const CUtensorMap *map;
@@ -136,7 +136,7 @@ __device__ __forceinline__ Item decode_job(const Job &j, int u) {
   it.n = j.n;
   it.store = j.store;
   it.t0 = j.t0;
-  it.words = j.words;
+  it.pad = 0;
   it.nbaseline = j.nbaseline;
   it.state = j.state;
   it.map = &j.map;
@@ -529,8 +529,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
             epi_barrier();
           }
-          uint8_t *srow = t.words ? sstate + il * kPitchWords + (p1 * 2 + c) * 8
-                                  : sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+          uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
           int jmax = t.n - cb * kStations;
           if (jmax > kStations) jmax = kStations;
           if (cb == rb && il + 1 < jmax) jmax = il + 1;
@@ -549,10 +548,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
               const long long re = unscale<kPacked>(c ? (long long)ra + v3 : (long long)v0 + rb2);
               const long long im = unscale<kPacked>(c ? (long long)v2 - rb2 : (long long)ra - v1);
               const int jl = q * 8 + jj;
-              if (jl < jmax) {
-                if (t.words) *(long long *)(srow + jl * 32) = visibility_word(re, im);
-                else *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
-              }
+              if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
             }
           }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -565,13 +561,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             if (cb == rb && lane + 1 < cnt) cnt = lane + 1;
             if (ig >= t.n) cnt = 0;
             if (cnt > 0) {
-              // int64 pairs (64 bytes per baseline) or words (32 bytes)
               int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
-                                        (long long)cb * kStations) * (t.words ? 4 : 8);
-              const uint32_t src = smem_u32(sstate + lane * (t.words ? kPitchWords : kRowPitch));
-              const uint32_t nb = (uint32_t)cnt * (t.words ? 32 : 64);
-              if (t.store) bulk_store(dst, src, nb);
-              else bulk_reduce_add(dst, src, nb);
+                                        (long long)cb * kStations) * 8;
+              const uint32_t src = smem_u32(sstate + lane * kRowPitch);
+              if (t.store) bulk_store(dst, src, cnt * 64);
+              else bulk_reduce_add(dst, src, cnt * 64);
             }
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
@@ -611,8 +605,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
         const int hlast = (2 * t.C + 1 > rb) ? 0 : 1;   // last column block at or below the diagonal
         for (int h = 0; h <= hlast; ++h) {
           const int cb = 2 * t.C + h;
-          uint8_t *srow = t.words ? sstate + il * kPitchWords + (p1 * 2 + c) * 8
-                                  : sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+          uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
           int jmax = t.n - cb * kStations;
           if (jmax > kStations) jmax = kStations;
           if (cb == rb && il + 1 < jmax) jmax = il + 1;
@@ -640,10 +633,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
               const long long re = unscale<kPacked>(c ? (long long)ra + v3 : (long long)v0 + rb2);
               const long long im = unscale<kPacked>(c ? (long long)v2 - rb2 : (long long)ra - v1);
               const int jl = q * 8 + jj;
-              if (jl < jmax) {
-                if (t.words) *(long long *)(srow + jl * 32) = visibility_word(re, im);
-                else *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
-              }
+              if (jl < jmax) *(longlong2 *)(srow + jl * 64) = make_longlong2(re, im);
             }
           }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -656,11 +646,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             if (ig >= t.n) cnt = 0;
             if (cnt > 0) {
               int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
-                                        (long long)cb * kStations) * (t.words ? 4 : 8);
-              const uint32_t src = smem_u32(sstate + crow * (t.words ? kPitchWords : kRowPitch));
-              const uint32_t nb = (uint32_t)cnt * (t.words ? 32 : 64);
-              if (t.store) bulk_store(dst, src, nb);
-              else bulk_reduce_add(dst, src, nb);
+                                        (long long)cb * kStations) * 8;
+              const uint32_t src = smem_u32(sstate + crow * kRowPitch);
+              if (t.store) bulk_store(dst, src, cnt * 64);
+              else bulk_reduce_add(dst, src, cnt * 64);
             }
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
@@ -721,7 +710,7 @@ cudaError_t tc2_set_smem_attribute() {
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap,
-                       int f0, int fcount, int packed, int words) {
+                       int f0, int fcount, int packed) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   const int num_sms = current_device_sms();
@@ -741,14 +730,12 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   ksplit = (total_steps + per - 1) / per;
   if ((long long)fcount * npairs * ksplit > 0x7fffffffLL) return cudaErrorInvalidValue;
   if (overwrite && ksplit > 1) {
-    // int64 values per channel: (re, im) pairs, or one word per visibility
-    const size_t per_channel = (size_t)s.state_elems / s.f / (words ? 2 : 1);
+    const size_t per_channel = (size_t)s.state_elems / s.f;   // int64 words
     cudaError_t e = cudaMemsetAsync(state + (size_t)f0 * per_channel, 0,
                                     (size_t)fcount * per_channel * 8, st);
     if (e != cudaSuccess) return e;
   }
   j.state = state;
-  j.words = words ? 1 : 0;
   j.nbaseline = s.nbaseline;
   j.n = s.n;
   j.f = fcount;

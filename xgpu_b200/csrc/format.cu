@@ -174,25 +174,6 @@ __global__ void generate_kernel(int8_t *out, unsigned long long nbytes, const Ge
       out[n] = gen_byte(g, thr, n);
 }
 
-// Adds a short-term word buffer into the int64 integration buffer: word k is
-// im * 2^32 + re of visibility k with |re|, |im| < 2^31, so its low 32 bits
-// read as a signed int32 are re, and (word - re) / 2^32 is im.  Two words per
-// thread (16-byte loads, 32-byte read-modify-writes of the buffer).
-__global__ void fold_words_kernel(const longlong2 *words, longlong4 *state, long long npairs) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npairs;
-       q += (long long)gridDim.x * blockDim.x) {
-    const longlong2 w = words[q];
-    const long long re0 = (long long)(int)(unsigned)(unsigned long long)w.x;
-    const long long re1 = (long long)(int)(unsigned)(unsigned long long)w.y;
-    longlong4 v = state[q];
-    v.x += re0;
-    v.y += (w.x - re0) >> 32;
-    v.z += re1;
-    v.w += (w.y - re1) >> 32;
-    state[q] = v;
-  }
-}
-
 static unsigned grid_for(long long work, int threads) {
   long long b = (work + threads - 1) / threads;
   if (b > 148LL * 16) b = 148LL * 16;
@@ -221,14 +202,6 @@ cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s,
                 (uint32_t *)out, f0 * per_ch, (f0 + fcount) * per_ch};
   const long long work = fcount * per_ch;
   fmt::format_kernel<<<fmt::grid_for(work, 256), 256, 0, st>>>(p);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_fold_words(const int64_t *words, int64_t *state, long long nwords,
-                              cudaStream_t st) {
-  if (nwords % 2) return cudaErrorInvalidValue;   // 4 polarisation products per baseline
-  fmt::fold_words_kernel<<<fmt::grid_for(nwords / 2, 256), 256, 0, st>>>(
-      (const longlong2 *)words, (longlong4 *)state, nwords / 2);
   return cudaGetLastError();
 }
 

@@ -92,17 +92,14 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 // or clears, that channel range only.
 // packed = 1: `map` describes packed 4+4-bit input (make_packed_map), which
 // the CTA-pair kernel expands in shared memory; it needs tune.wide.
-// words = 1: `state` is a short-term buffer of one int64 word per visibility,
-// im * 2^32 + re (tri_length words; Job::words), which holds at most
-// kWordSamples samples before fold_words must add it into the int64 buffer.
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
                             const TcTuning &tune, int overlap, int f0 = 0, int fcount = -1,
-                            int packed = 0, int words = 0);
+                            int packed = 0);
 // The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune,
-                       int overlap, int f0 = 0, int fcount = -1, int packed = 0, int words = 0);
+                       int overlap, int f0 = 0, int fcount = -1, int packed = 0);
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
@@ -150,10 +147,6 @@ cudaError_t launch_format(const void *state, int state_is_float, const Sizes &s,
                           int fcount = -1);
 cudaError_t launch_generate(void *out, size_t nbytes, int kind, unsigned long long seed,
                             double sigma, cudaStream_t st);
-// state[2k] += re, state[2k+1] += im of each of the nwords words
-// im * 2^32 + re of a short-term buffer (see kWordSamples).
-cudaError_t launch_fold_words(const int64_t *words, int64_t *state, long long nwords,
-                              cudaStream_t st);
 
 // Host Gaussian table shared with the generator kernel.
 void gauss_thresholds(double sigma, uint32_t thr[254]);

@@ -86,16 +86,6 @@ struct Internal {
   // of device-resident input here (on s_conv) before converting them.
   void *d_slice = nullptr;
   void *d_state = nullptr;             // integration buffer
-  // Tensor engine: adding launches over a context's calls reduce-add one
-  // int64 word per visibility, im * 2^32 + re, into this short-term buffer
-  // (half the bytes and half the elements of the int64 (re, im) pairs: the
-  // epilogue's bulk reduce-adds are what an accumulating call at moderate N
-  // waits for); it is folded into d_state before any read of the sums and
-  // before it holds kWordSamples samples.  Stores after a clear, and dumping
-  // calls over host buffers, go to d_state directly.
-  int64_t *d_words = nullptr;
-  bool words_zero = true;          // the word buffer holds nothing (the next launch stores)
-  long long words_samples = 0;     // samples added since it was last folded
   void *d_out = nullptr;               // formatted dump
   int *d_err = nullptr;                // device error word
   int *h_err = nullptr;                // pinned copy of it
@@ -212,7 +202,6 @@ int free_device(Internal *in) {
   if (in->caller_ev) cudaEventDestroy(in->caller_ev);
   if (in->d_slice) cudaFree(in->d_slice);
   if (in->d_state) cudaFree(in->d_state);
-  if (in->d_words) cudaFree(in->d_words);
   if (in->d_out) cudaFree(in->d_out);
   if (in->d_err) cudaFree(in->d_err);
   if (in->h_err) cudaFreeHost(in->h_err);
@@ -268,27 +257,15 @@ bool packed_in_kernel(const Internal *in) {
          in->cfg.engine == XGPU_ENGINE_TENSOR && in->tune.wide;
 }
 
-// Add the short-term word buffer into the integration buffer (queued on
-// s_comp after every launch that wrote it) and mark it empty.
-int fold_words(Internal *in) {
-  if (in->words_zero) return XGPU_OK;
-  XGPU_CHECK(launch_fold_words(in->d_words, (int64_t *)in->d_state, in->sz.tri_length, in->s_comp));
-  in->words_zero = true;
-  in->words_samples = 0;
-  in->adding_tail = false;
-  return XGPU_OK;
-}
-
 // Queue the engine over channels [f0, f0 + fcount) of int8 input x (packed
 // input when `packed`: packed_in_kernel) on s_comp, in time segments; the
 // first segment stores when the buffer is known to be zero.  x has geometry s
 // (in->szc for the context's compact buffers, in->sz for a full-band device
 // input read in place, x then pointing at the context's first channel).
 // *tail: in, the launch may overlap the adding launch before it; out, the
-// last launch queued only added.  use_words: the tensor engine's adding
-// launches go to the short-term word buffer (the whole band of channels).
+// last launch queued only added.
 int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fcount, bool *tail,
-                  bool packed = false, bool use_words = false) {
+                  bool packed = false) {
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
     XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
@@ -307,23 +284,10 @@ int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fco
     }
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      int store = ow && t0 == 0;
-      int64_t *target = (int64_t *)in->d_state;
-      int words = 0;
-      if (!store && use_words && in->d_words) {
-        if (in->words_samples + tc > kWordSamples) {
-          const int r = fold_words(in);
-          if (r != XGPU_OK) return r;
-          *tail = false;   // the fold sits between this launch and the last
-        }
-        target = in->d_words;
-        words = 1;
-        store = in->words_zero ? 1 : 0;
-        in->words_zero = false;
-        in->words_samples += tc;
-      }
-      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, target, store, in->d_err, in->s_comp, in->tune,
-                                 *tail && !store ? 1 : 0, f0, fcount, packed ? 1 : 0, words));
+      const int store = ow && t0 == 0;
+      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
+                                 in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount,
+                                 packed ? 1 : 0));
       *tail = !store;   // the next segment follows an adding launch
     }
   }
@@ -386,7 +350,7 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready, bool 
       geom = &in->sz;
     }
   }
-  const int r = launch_engine(in, x, *geom, 0, s.f, &tail, packed, true);
+  const int r = launch_engine(in, x, *geom, 0, s.f, &tail, packed);
   if (r != XGPU_OK) return r;
   if (in->int_state && in->cfg.engine == XGPU_ENGINE_TENSOR) in->adding_tail = tail && conv < 0;
   in->state_zero = false;
@@ -439,10 +403,6 @@ int dump(XGPUContext *ctx, Internal *in) {
   if (in->state_zero) {
     XGPU_CHECK(cudaMemsetAsync(in->d_state, 0, (size_t)in->sz.state_elems * (in->int_state ? 8 : 4),
                                in->s_comp));
-  }
-  {
-    const int r = fold_words(in);
-    if (r != XGPU_OK) return r;
   }
   void *direct = direct_output(ctx, in);
   XGPU_CHECK(launch_format(in->d_state, in->int_state ? 0 : 1, in->sz, in->cfg.matrix_order,
@@ -513,12 +473,6 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
       bound[++ng] = f;
     }
     bound[++ng] = s.f;
-  }
-  // The channel groups add into the integration buffer itself, which the
-  // formatting reads: earlier calls' short-term sums go in first.
-  {
-    const int r = fold_words(in);
-    if (r != XGPU_OK) return r;
   }
   // The buffer is free once the engine launch that last read it has finished.
   XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
@@ -737,8 +691,6 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
   if (cudaMalloc(&in->d_in[0], in_bytes) != cudaSuccess ||
       cudaMalloc(&in->d_in[1], in_bytes) != cudaSuccess ||
       cudaMalloc(&in->d_state, state_bytes) != cudaSuccess ||
-      (in->int_state && cfg.engine == XGPU_ENGINE_TENSOR &&
-       cudaMalloc((void **)&in->d_words, (size_t)s.tri_length * 8) != cudaSuccess) ||
       cudaMalloc(&in->d_out, (size_t)s.mat_length * sizeof(Complex)) != cudaSuccess ||
       cudaMalloc(&in->d_err, sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&in->h_err, sizeof(int)) != cudaSuccess ||
@@ -803,8 +755,6 @@ int xgpuClearDeviceIntegrationBuffer(XGPUContext *context) {
   XGPU_CHECK(cudaSetDevice(in->device));
   // Ordered after queued engine launches; the next launch overwrites.
   in->state_zero = true;
-  in->words_zero = true;
-  in->words_samples = 0;
   return XGPU_OK;
 }
 
@@ -964,10 +914,6 @@ int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_o
     memset(host_out, 0, bytes);
     return check_device_error(in);
   }
-  {
-    const int r = fold_words(in);
-    if (r != XGPU_OK) return r;
-  }
   XGPU_CHECK(cudaMemcpyAsync(host_out, in->d_state, bytes, cudaMemcpyDeviceToHost, in->s_comp));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
   return check_device_error(in);
@@ -1062,16 +1008,13 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
     t.wide = cands[ci].wide;
     t.streamk = cands[ci].streamk;
     // Timed as calls run: on the context's own stream an accumulating launch
-    // overlaps the previous one (the first launch of a candidate does not),
-    // and adds into the short-term word buffer (the scratch buffer's sums are
-    // never read).
+    // overlaps the previous one (the first launch of a candidate does not).
     const int chain = in->s_comp == in->s_own ? 1 : 0;
-    const int words = in->d_words ? 1 : 0;
     auto run = [&](int overlap) {
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
         if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t,
-                            overlap, 0, -1, 0, words) != cudaSuccess)
+                            overlap) != cudaSuccess)
           return false;
         overlap = chain;
       }

@@ -181,20 +181,6 @@ __device__ __forceinline__ void pdl_wait() {
 
 constexpr int kEpiThreads = 128;   // four epilogue warps, one per TMEM lane quarter
 
-// Staging of drained sums, one row per station of a 32-station block, 32
-// baselines x 4 polarisation products per row.  Pairs format: int64 (re, im)
-// (2 KB per row, 16 bytes of padding); word format (Job::words): one int64
-// word im * 2^32 + re per visibility (1 KB per row, 32 bytes of padding, so
-// the four stations that a half-warp's 8-byte stores reach start 32 bytes
-// apart in the banks).
-constexpr int kPitchPairs = 32 * 64 + 16;
-constexpr int kPitchWords = 32 * 32 + 32;
-
-// The word of a visibility's sums (|re|, |im| < 2^31): exact in int64.
-__device__ __forceinline__ long long visibility_word(long long re, long long im) {
-  return im * 4294967296LL + re;
-}
-
 __device__ __forceinline__ void epi_barrier() {
   asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
 }

@@ -26,16 +26,7 @@ struct Job {
   int items;              // f * npairs * ksplit
   int item_begin;         // first work item of this job in the launch
   int store;              // 1: sole writer of a zero buffer (store); 0: reduce-add
-  int words;              // 1: state is a short-term buffer of one int64 word per
-                          // visibility, im * 2^32 + re (see kWordSamples)
 };
-
-// Samples a short-term word buffer may hold before it must be folded into the
-// int64 integration buffer.  One sample adds at most 2 * 128 * 128 = 2^15 in
-// magnitude to a real or imaginary part, so after at most 65535 samples both
-// sums stay inside int32 and the sum of the words im * 2^32 + re (exact in
-// 64-bit two's complement) still separates into them.
-constexpr int kWordSamples = 65520;
 
 struct TcTuning {
   int ksplit = 1;         // time splits per tile (1 = none)
