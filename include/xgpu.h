@@ -332,8 +332,11 @@ int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGP
  * every tile's samples into that many items whose partial sums are added
  * exactly in the integration buffer; grid is the number of CTAs (0 = one per
  * SM).  ksplit = 0 autotunes all three now: the engine is timed on synthetic
- * input and a scratch integration buffer (the context's own is not touched)
- * and the fastest setting is kept.  With CTA pairs, XGPU_INPUT_PACKED4 input
+ * input and a scratch integration buffer (the context's own is not touched),
+ * in chains of calls that overlap as a stream of calls does and read their
+ * input from device memory rather than the L2 cache (temporary buffers of up
+ * to about 256 MB plus one integration buffer, freed before it returns), and
+ * the fastest setting is kept.  With CTA pairs, XGPU_INPUT_PACKED4 input
  * is expanded inside the kernel; the other kernels read an int8 copy that a
  * pre-pass makes. */
 int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair);

@@ -177,22 +177,26 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
       r[1] = rw[g * kBlk + 16 + ty];
       c[0] = cw[g * kBlk + tx];
       c[1] = cw[g * kBlk + 16 + tx];
+      // Four sweeps over the 16 visibilities of the 2x2 tile, so that the two
+      // dp4a of one real part are 48 instructions apart, not back to back.
 #pragma unroll
-      for (int rs = 0; rs < 2; ++rs)
+      for (int sweep = 0; sweep < 4; ++sweep)
 #pragma unroll
-        for (int cs = 0; cs < 2; ++cs) {
-          const int ar[2] = {r[rs].x, r[rs].z}, ai[2] = {r[rs].y, r[rs].w};
-          const int br[2] = {c[cs].x, c[cs].z}, bi[2] = {c[cs].y, c[cs].w};
+        for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
-          for (int p1 = 0; p1 < 2; ++p1)
+          for (int cs = 0; cs < 2; ++cs) {
+            const int ar[2] = {r[rs].x, r[rs].z}, ai[2] = {r[rs].y, r[rs].w};
+            const int br[2] = {c[cs].x, c[cs].z}, bi[2] = {c[cs].y, c[cs].w};
 #pragma unroll
-            for (int p2 = 0; p2 < 2; ++p2) {
-              re[rs][cs][p1][p2] = dp4a(ar[p1], br[p2], re[rs][cs][p1][p2]);
-              re[rs][cs][p1][p2] = dp4a(ai[p1], bi[p2], re[rs][cs][p1][p2]);
-              i1[rs][cs][p1][p2] = dp4a(ai[p1], br[p2], i1[rs][cs][p1][p2]);
-              i2[rs][cs][p1][p2] = dp4a(ar[p1], bi[p2], i2[rs][cs][p1][p2]);
-            }
-        }
+            for (int p1 = 0; p1 < 2; ++p1)
+#pragma unroll
+              for (int p2 = 0; p2 < 2; ++p2) {
+                if (sweep == 0) re[rs][cs][p1][p2] = dp4a(ar[p1], br[p2], re[rs][cs][p1][p2]);
+                if (sweep == 1) i1[rs][cs][p1][p2] = dp4a(ai[p1], br[p2], i1[rs][cs][p1][p2]);
+                if (sweep == 2) i2[rs][cs][p1][p2] = dp4a(ar[p1], bi[p2], i2[rs][cs][p1][p2]);
+                if (sweep == 3) re[rs][cs][p1][p2] = dp4a(ai[p1], bi[p2], re[rs][cs][p1][p2]);
+              }
+          }
     }
     __syncthreads();
   }

@@ -64,17 +64,30 @@ constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kThreads = 192;
 constexpr uint32_t kIdesc = i8_idesc(2 * kHalf, 2 * kHalf);
 // Packed 4+4-bit input (one byte per complex sample, 2n bytes per sample):
-// each CTA loads its 32 stations' packed bytes (64 per sample) into the upper
-// half of an operand box, and converter warps expand them in place into the
-// int8 layout the MMA reads.  One converter warp owns each pipeline slot, so
-// every slot's phases are waited on in order.
-constexpr int kPackedRow = kStations * 2;     // 64 packed bytes per sample
-constexpr int kPackedBox = kPackedRow * kKt;  // 8 KiB
-constexpr int kConvWarps = kStages;
+// the producer loads each CTA's packed boxes (64 bytes per sample row: 32
+// stations) with TMA into a ring of kPackedSlots slots of its own, and
+// kConvWarps converter warps expand every stage from there into an operand
+// ring of kStagesPacked stages -- the two rings take the shared memory of the
+// int8 kernel's kStages stages.  Each converter warp owns 32 sample rows of
+// both boxes of every stage, so a stage's expansion is spread over four warps
+// and the packed loads run up to kPackedSlots stages ahead of it.
+constexpr int kPackedRow = kStations * 2;                // 64 packed bytes per sample
+constexpr int kPackedBox = kPackedRow * kKt;             // 8 KiB
+constexpr int kPackedSlotBytes = 2 * kPackedBox;         // A and B boxes
+constexpr int kStagesPacked = 3;
+constexpr int kPackedSlots = 4;
+static_assert(kStagesPacked * kStageBytes + kPackedSlots * kPackedSlotBytes <= kStages * kStageBytes,
+              "the packed rings fit the int8 kernel's stages");
+constexpr int kConvWarps = 4;
+static_assert(kConvWarps * 32 == kKt, "32 sample rows per converter warp");
 constexpr int kThreadsPacked = kThreads + 32 * kConvWarps;
-// barriers (24 slots), work-item ring, TMEM slot and abort flag, then the
-// packed-input slot barriers and slot contents
-static_assert(24 * 8 + kSched * 64 + 8 + kStages * 9 <= kBarrierBytes, "barrier area");
+// barriers (full/empty per stage, 2 x 2 accumulator, ring, mma_done, one
+// spare), work-item ring, TMEM slot and abort flag; packed input adds its
+// slots' loaded/free barriers and contents
+static_assert((2 * kStages + 6 + 2 * kSched) * 8 + kSched * 64 + 8 <= kBarrierBytes, "barriers");
+static_assert((2 * kStagesPacked + 6 + 2 * kSched) * 8 + kSched * 64 + 8 + kPackedSlots * 17 <=
+                  kBarrierBytes,
+              "barriers of the packed instantiation");
 
 struct Params {
   Job job;             // the job when jobs == nullptr (npairs counts 256x256 tiles)
@@ -239,27 +252,34 @@ __device__ __forceinline__ long long unscale(long long v) {
   return kPacked ? v >> 8 : v;   // exact: every packed-input sum is a multiple of 256
 }
 
-// Expands, in place, the packed panel that TMA wrote into the upper half of a
-// 16 KiB operand box (128 samples x 64 bytes) into the box itself: 128 samples
-// x 128 int8 bytes in the 128-byte swizzled layout (16-byte chunk j of sample
-// row r at r*128 + ((j ^ (r & 7)) << 4)).  In pass q, lane l makes chunk
-// j = l%8 of row r = 4q + l/8 from the row's packed bytes 8j .. 8j+7, so each
-// group of eight lanes reads 64 consecutive bytes and writes the eight chunks
-// of one row (all 32 banks once).  Every lane reads all its packed bytes
-// before any lane writes, so no packed byte is overwritten before it is read.
-__device__ __forceinline__ void expand_box(uint8_t *box, int lane) {
-  const uint8_t *packed = box + kPackedBox;
-  const int j = lane & 7;
-  uint2 w[kKt / 4];
+// A converter warp's share of one packed box in shared memory (64 bytes per
+// sample row): rows r0 .. r0 + 31.  Lane l reads 16 bytes -- part m = l % 4 of
+// row r0 + 8k + l / 4 -- in each of four loads k (each load reads eight whole
+// rows: 512 contiguous bytes, conflict-free).
+__device__ __forceinline__ void load_packed_rows(const uint8_t *pbox, int r0, int lane,
+                                                 uint4 (&v)[4]) {
 #pragma unroll
-  for (int q = 0; q < kKt / 4; ++q)
-    w[q] = *(const uint2 *)(packed + (4 * q + (lane >> 3)) * kPackedRow + j * 8);
-  __syncwarp();
+  for (int k = 0; k < 4; ++k)
+    v[k] = *(const uint4 *)(pbox + (r0 + 8 * k + (lane >> 2)) * kPackedRow + 16 * (lane & 3));
+}
+
+// Expands what load_packed_rows read into rows r0 .. r0 + 31 of a 16 KiB
+// operand box: 128 int8 bytes per row in the 128-byte swizzled layout
+// (16-byte chunk j of row r at r*128 + ((j ^ (r & 7)) << 4)).  Part m of a row
+// becomes chunks 2m and 2m + 1.  A quarter-warp's eight lanes hold the four
+// parts of two consecutive rows r (even) and r + 1: their even (odd) chunks
+// land on complementary halves of the banks, so each store is conflict-free.
+__device__ __forceinline__ void store_expanded_rows(uint8_t *box, int r0, int lane,
+                                                    const uint4 (&v)[4]) {
+  const int m = lane & 3;
 #pragma unroll
-  for (int q = 0; q < kKt / 4; ++q) {
-    const int r = 4 * q + (lane >> 3);
-    const uint2 e0 = expand_scaled(w[q].x), e1 = expand_scaled(w[q].y);
-    *(uint4 *)(box + r * 128 + ((j ^ (r & 7)) << 4)) = make_uint4(e0.x, e0.y, e1.x, e1.y);
+  for (int k = 0; k < 4; ++k) {
+    const int r = r0 + 8 * k + (lane >> 2);
+    const uint2 e0 = expand_scaled(v[k].x), e1 = expand_scaled(v[k].y);
+    const uint2 e2 = expand_scaled(v[k].z), e3 = expand_scaled(v[k].w);
+    uint8_t *row = box + r * 128;
+    *(uint4 *)(row + (((2 * m) ^ (r & 7)) << 4)) = make_uint4(e0.x, e0.y, e1.x, e1.y);
+    *(uint4 *)(row + (((2 * m + 1) ^ (r & 7)) << 4)) = make_uint4(e2.x, e2.y, e3.x, e3.y);
   }
 }
 
@@ -274,21 +294,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
     xengine_tc2_kernel(const __grid_constant__ Params p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  // operand stages the MMA reads (packed input: the rest of the int8
+  // kernel's stage memory holds the packed slots)
+  constexpr int S = kPacked ? kStagesPacked : kStages;
   uint8_t *sstate = smem + kStages * kStageBytes;
+  uint8_t *packed_slots = smem + S * kStageBytes;   // kPacked only
   uint64_t *bars = (uint64_t *)(sstate + kStateBytes);
-  // full[kStages] empty[kStages] tfull[2] tempty[2] sfull[kSched] sempty[kSched] mma_done
-  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
-                 tfull0 = smem_u32(bars + 2 * kStages), tempty0 = smem_u32(bars + 2 * kStages + 2),
-                 sfull0 = smem_u32(bars + 2 * kStages + 4),
-                 sempty0 = smem_u32(bars + 2 * kStages + 4 + kSched),
-                 mma_done = smem_u32(bars + 2 * kStages + 4 + 2 * kSched);
-  Item *ring = (Item *)(bars + 2 * kStages + 6 + 2 * kSched);
+  // full[S] empty[S] tfull[2] tempty[2] sfull[kSched] sempty[kSched] mma_done
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + S),
+                 tfull0 = smem_u32(bars + 2 * S), tempty0 = smem_u32(bars + 2 * S + 2),
+                 sfull0 = smem_u32(bars + 2 * S + 4),
+                 sempty0 = smem_u32(bars + 2 * S + 4 + kSched),
+                 mma_done = smem_u32(bars + 2 * S + 4 + 2 * kSched);
+  Item *ring = (Item *)(bars + 2 * S + 6 + 2 * kSched);
   uint32_t *tmem_slot = (uint32_t *)(ring + kSched);
   volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
-  // packed input: the slots' packed-load barriers, and each slot's content
+  // packed input: each slot's "loaded" barrier (the producer's TMA bytes) and
+  // "free" barrier (every converter warp has read it), and its content
   // (0: A and B boxes, 1: A only (diagonal tile), -1: no more stages)
-  const uint32_t raw0 = smem_u32(tmem_slot + 2);
-  volatile signed char *stage_info = (volatile signed char *)(tmem_slot + 2 + 2 * kStages);
+  const uint32_t praw0 = smem_u32(tmem_slot + 2), pfree0 = praw0 + 8 * kPackedSlots;
+  volatile signed char *slot_info = (volatile signed char *)(tmem_slot + 2 + 4 * kPackedSlots);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_rank();
@@ -303,12 +328,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < S; ++s) {
       // int8 input: the leader's arrival, and both CTAs' loads complete on it;
-      // packed input: one converter warp of each CTA
-      mbar_init(full0 + 8 * s, kPacked ? 2 : 1);
+      // packed input: every converter warp of both CTAs
+      mbar_init(full0 + 8 * s, kPacked ? 2 * kConvWarps : 1);
       mbar_init(empty0 + 8 * s, 1);
-      if (kPacked) mbar_init(raw0 + 8 * s, 1);
+    }
+    if (kPacked) {
+      for (int q = 0; q < kPackedSlots; ++q) {
+        mbar_init(praw0 + 8 * q, 1);
+        mbar_init(pfree0 + 8 * q, kConvWarps);
+      }
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(tfull0 + 8 * a, 1);
@@ -381,27 +411,38 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
         if (t.u >= p.total) break;
         const bool diag = (t.R == t.C);
         const int rb = 2 * t.R + (int)rank, cbb = 2 * t.C + (int)rank;
-        for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
-          const uint32_t s = g % kStages;
-          if (g >= (uint32_t)kStages &&
-              !mbar_wait(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort_flag)) {
-            fail(kErrTimeoutProducer);
-            ok = false;
-            break;
-          }
-          if (p.stall) continue;
-          const uint32_t dst = stage0 + s * kStageBytes;
-          const int z = t.t0 + (t.step0 + ks) * kKt;
-          if (kPacked) {
-            // this CTA's packed rows into the upper halves of its boxes, for
-            // its own converter warp
-            stage_info[s] = diag ? 1 : 0;
-            mbar_expect_tx(raw0 + 8 * s, diag ? kPackedBox : 2 * kPackedBox);
-            tma_load_3d(dst + kPackedBox, t.map, raw0 + 8 * s, rb * kPackedRow, t.f, z);
+        if (kPacked) {
+          // this CTA's packed boxes into the next packed slot, for the
+          // converter warps of this CTA
+          for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
+            const uint32_t q = g % kPackedSlots;
+            if (g >= (uint32_t)kPackedSlots &&
+                !mbar_wait(pfree0 + 8 * q, ((g / kPackedSlots) - 1) & 1, abort_flag)) {
+              fail(kErrTimeoutProducer);
+              ok = false;
+              break;
+            }
+            if (p.stall) continue;
+            const uint32_t dst = smem_u32(packed_slots + q * kPackedSlotBytes);
+            const int z = t.t0 + (t.step0 + ks) * kKt;
+            slot_info[q] = diag ? 1 : 0;
+            mbar_expect_tx(praw0 + 8 * q, diag ? kPackedBox : 2 * kPackedBox);
+            tma_load_3d(dst, t.map, praw0 + 8 * q, rb * kPackedRow, t.f, z);
             if (!diag)
-              tma_load_3d(dst + kBoxBytes + kPackedBox, t.map, raw0 + 8 * s, cbb * kPackedRow,
-                          t.f, z);
-          } else {
+              tma_load_3d(dst + kPackedBox, t.map, praw0 + 8 * q, cbb * kPackedRow, t.f, z);
+          }
+        } else {
+          for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
+            const uint32_t s = g % S;
+            if (g >= (uint32_t)S &&
+                !mbar_wait(empty0 + 8 * s, ((g / S) - 1) & 1, abort_flag)) {
+              fail(kErrTimeoutProducer);
+              ok = false;
+              break;
+            }
+            if (p.stall) continue;
+            const uint32_t dst = stage0 + s * kStageBytes;
+            const int z = t.t0 + (t.step0 + ks) * kKt;
             const uint32_t fbar = peer_addr(full0 + 8 * s, 0);
             // The leader expects the bytes of both CTAs; the peer's loads may land
             // first (the transaction count then dips below zero until it does).
@@ -411,17 +452,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
           }
         }
       }
-      if (kPacked && !p.stall) {
-        // No stage follows: tell each converter warp, in its slot's next phase.
-        for (int e = 0; e < kConvWarps && !*abort_flag; ++e, ++g) {
-          const uint32_t s = g % kStages;
-          if (g >= (uint32_t)kStages &&
-              !mbar_wait(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort_flag)) {
-            fail(kErrTimeoutProducer);
-            break;
-          }
-          stage_info[s] = -1;
-          mbar_arrive(raw0 + 8 * s);
+      if (kPacked && ok && !p.stall) {
+        // No stage follows: one slot says so to every converter warp.
+        const uint32_t q = g % kPackedSlots;
+        if (g < (uint32_t)kPackedSlots ||
+            mbar_wait(pfree0 + 8 * q, ((g / kPackedSlots) - 1) & 1, abort_flag)) {
+          slot_info[q] = -1;
+          mbar_arrive(praw0 + 8 * q);
+        } else {
+          fail(kErrTimeoutProducer);
         }
       }
     }
@@ -449,10 +488,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + (uint32_t)(acc * kAccCols);
         for (int ks = 0; ks < t.nsteps; ++ks, ++g) {
-          const uint32_t s = g % kStages;
+          const uint32_t s = g % S;
           // packed input: both CTAs' converters arrived (the peer's from its CTA)
-          if (!(kPacked ? mbar_wait_cluster(full0 + 8 * s, (g / kStages) & 1, abort_flag)
-                        : mbar_wait(full0 + 8 * s, (g / kStages) & 1, abort_flag))) {
+          if (!(kPacked ? mbar_wait_cluster(full0 + 8 * s, (g / S) & 1, abort_flag)
+                        : mbar_wait(full0 + 8 * s, (g / S) & 1, abort_flag))) {
             fail(kErrTimeoutMma);
             ok = false;
             break;
@@ -659,28 +698,42 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
     }
   } else {
     // -------------------------------------------------------- converters --
-    // Packed input only.  Converter warp w owns pipeline slot w: for each of
-    // the slot's stages it waits for this CTA's packed loads, expands the A
-    // box (and the B box off the diagonal) in place, makes the bytes visible
-    // to the tensor cores and reports the stage on the leader's barrier.
-    const int w = warp - 6;
-    const uint32_t fullw = leader ? full0 + 8 * w : peer_addr(full0 + 8 * w, 0);
-    for (uint32_t k = 0;; ++k) {
-      const bool got = mbar_wait(raw0 + 8 * w, k & 1, abort_flag);
-      if (!__all_sync(0xffffffffu, got)) {
+    // Packed input only.  Converter warp w expands sample rows 32w .. 32w + 31
+    // of both boxes of every stage: it waits for the stage's packed slot and
+    // for its operand stage to be free (the MMA has read it), expands its rows
+    // into it, makes them visible to the tensor cores, reports on the leader's
+    // "full" barrier and frees its share of the packed slot.
+    const int r0 = (warp - 6) * 32;
+    for (uint32_t g = 0;; ++g) {
+      const uint32_t q = g % kPackedSlots;
+      if (!__all_sync(0xffffffffu,
+                      mbar_wait(praw0 + 8 * q, (g / kPackedSlots) & 1, abort_flag))) {
         if (lane == 0) fail(kErrTimeoutConvert);
         break;
       }
-      const int info = stage_info[w];
+      const int info = slot_info[q];
       if (info < 0) break;
-      uint8_t *box = smem + w * kStageBytes;
-      expand_box(box, lane);
-      if (info == 0) expand_box(box + kBoxBytes, lane);
+      const uint32_t s = g % S;
+      if (g >= (uint32_t)S &&
+          !__all_sync(0xffffffffu, mbar_wait(empty0 + 8 * s, ((g / S) - 1) & 1, abort_flag))) {
+        if (lane == 0) fail(kErrTimeoutConvert);
+        break;
+      }
+      const uint8_t *pk = packed_slots + q * kPackedSlotBytes;
+      uint8_t *box = smem + s * kStageBytes;
+      uint4 v[4];
+      load_packed_rows(pk, r0, lane, v);
+      store_expanded_rows(box, r0, lane, v);
+      if (info == 0) {
+        load_packed_rows(pk + kPackedBox, r0, lane, v);
+        store_expanded_rows(box + kBoxBytes, r0, lane, v);
+      }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) {
-        if (leader) mbar_arrive(fullw);
-        else remote_arrive(fullw);
+        if (leader) mbar_arrive(full0 + 8 * s);
+        else remote_arrive(peer_addr(full0 + 8 * s, 0));
+        mbar_arrive(pfree0 + 8 * q);
       }
     }
   }
@@ -710,9 +763,10 @@ cudaError_t tc2_set_smem_attribute() {
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap,
-                       int f0, int fcount, int packed) {
+                       int f0, int fcount, const void *packed_in) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
+  const bool packed = packed_in != nullptr;   // `map` describes it (make_packed_map)
   const int num_sms = current_device_sms();
   if (!num_sms) return cudaErrorInvalidDevice;
   {

@@ -90,16 +90,18 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 // commuting.  Channels [f0, f0 + fcount) of the input and buffer are
 // correlated (fcount < 0: through the last channel); an overwrite stores into,
 // or clears, that channel range only.
-// packed = 1: `map` describes packed 4+4-bit input (make_packed_map), which
-// the CTA-pair kernel expands in shared memory; it needs tune.wide.
+// packed_in != nullptr: the input is packed 4+4-bit, at packed_in with
+// geometry s (the pointer `map` was made from with make_packed_map), and the
+// CTA-pair kernel loads and expands it itself; it needs tune.wide.
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
                             const TcTuning &tune, int overlap, int f0 = 0, int fcount = -1,
-                            int packed = 0);
+                            const void *packed_in = nullptr);
 // The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune,
-                       int overlap, int f0 = 0, int fcount = -1, int packed = 0);
+                       int overlap, int f0 = 0, int fcount = -1,
+                       const void *packed_in = nullptr);
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.
 cudaError_t launch_tc_batch(const Job *dev_jobs, int njobs, int total_items, int *queue, int *err,
