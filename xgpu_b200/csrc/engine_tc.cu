@@ -57,11 +57,8 @@ constexpr int kStages = 5;
 constexpr int kSched = 4;                  // work-item ring between the roles
 constexpr int kBoxBytes = kTile * kKt;     // one operand of one stage: 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;
-// One station row of the staging tile; 16 bytes of padding put the 8 rows a
-// warp writes on distinct 16-byte bank groups, and five 32 KB stages still
-// fit in 227 KB.
-constexpr int kRowPitch = kStations * 64 + 16;
-constexpr int kStateBytes = kStations * kRowPitch;
+// Staging of one 32x32-station block of drained sums (staging_row).
+constexpr int kStateBytes = kStagingBytes;
 constexpr int kBarrierBytes = 512;    // barriers, work-item ring, TMEM slot
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
 static_assert(kSmemBytes <= 227 * 1024, "dynamic shared memory of one CTA");
@@ -358,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       }
       __syncwarp();
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+      uint8_t *srow = sstate + staging_row(il) + (p1 * 2 + c) * 16;
       int jmax = t.n - t.tc * kStations;
       if (jmax > kStations) jmax = kStations;
       if (t.tr == t.tc && il + 1 < jmax) jmax = il + 1;
@@ -392,7 +389,7 @@ __global__ void __launch_bounds__(kThreads, 1) xengine_tc_kernel(const __grid_co
       if (copier) {
         const int nb = row_bytes(t, lane);
         if (nb) {
-          const uint32_t src = smem_u32(sstate + lane * kRowPitch);
+          const uint32_t src = smem_u32(sstate + staging_row(lane));
           if (t.store) bulk_store(row_ptr(t, lane), src, nb);
           else bulk_reduce_add(row_ptr(t, lane), src, nb);
         }

@@ -52,10 +52,8 @@ constexpr int kStages = 5;
 constexpr int kSched = 4;
 constexpr int kBoxBytes = kHalf * kKt;      // 16 KiB
 constexpr int kStageBytes = 2 * kBoxBytes;  // A rows + B half
-// 16 bytes of padding per 2 KB row: the 8 rows a warp writes fall on distinct
-// 16-byte bank groups, and five 32 KB stages still fit in 227 KB.
-constexpr int kRowPitch = kStations * 64 + 16;
-constexpr int kStateBytes = kStations * kRowPitch;   // one 32x32-station block
+// Staging of one 32x32-station block of drained sums (staging_row).
+constexpr int kStateBytes = kStagingBytes;
 constexpr int kBarrierBytes = 512;    // barriers, work-item ring, TMEM slot
 constexpr int kSmemBytes = kStages * kStageBytes + kStateBytes + kBarrierBytes + 1024;
 static_assert(kSmemBytes <= 227 * 1024, "dynamic shared memory of one CTA");
@@ -568,7 +566,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
             epi_barrier();
           }
-          uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+          uint8_t *srow = sstate + staging_row(il) + (p1 * 2 + c) * 16;
           int jmax = t.n - cb * kStations;
           if (jmax > kStations) jmax = kStations;
           if (cb == rb && il + 1 < jmax) jmax = il + 1;
@@ -602,7 +600,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             if (cnt > 0) {
               int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
                                         (long long)cb * kStations) * 8;
-              const uint32_t src = smem_u32(sstate + lane * kRowPitch);
+              const uint32_t src = smem_u32(sstate + staging_row(lane));
               if (t.store) bulk_store(dst, src, cnt * 64);
               else bulk_reduce_add(dst, src, cnt * 64);
             }
@@ -644,7 +642,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
         const int hlast = (2 * t.C + 1 > rb) ? 0 : 1;   // last column block at or below the diagonal
         for (int h = 0; h <= hlast; ++h) {
           const int cb = 2 * t.C + h;
-          uint8_t *srow = sstate + il * kRowPitch + (p1 * 2 + c) * 16;
+          uint8_t *srow = sstate + staging_row(il) + (p1 * 2 + c) * 16;
           int jmax = t.n - cb * kStations;
           if (jmax > kStations) jmax = kStations;
           if (cb == rb && il + 1 < jmax) jmax = il + 1;
@@ -686,7 +684,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             if (cnt > 0) {
               int64_t *dst = t.state + ((long long)t.f * t.nbaseline + ig * (ig + 1) / 2 +
                                         (long long)cb * kStations) * 8;
-              const uint32_t src = smem_u32(sstate + crow * kRowPitch);
+              const uint32_t src = smem_u32(sstate + staging_row(crow));
               if (t.store) bulk_store(dst, src, cnt * 64);
               else bulk_reduce_add(dst, src, cnt * 64);
             }

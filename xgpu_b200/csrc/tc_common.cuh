@@ -181,6 +181,15 @@ __device__ __forceinline__ void pdl_wait() {
 
 constexpr int kEpiThreads = 128;   // four epilogue warps, one per TMEM lane quarter
 
+// Staging of drained sums: one 2 KB row per station of a 32-station block (32
+// baselines x 4 polarisation products x int64 (re, im)), handed row by row to
+// the bulk-copy engine.  An epilogue warp's 16-byte stores reach two stations'
+// rows per quarter-warp (stations 2a and 2a + 1, one baseline, 64 bytes each).
+// Rows go in pairs of 4160 bytes, the odd row 2112 bytes after the even one:
+// 64 bytes apart in the banks, so the two segments fall on disjoint halves.
+__device__ __forceinline__ int staging_row(int il) { return (il >> 1) * 4160 + (il & 1) * 2112; }
+constexpr int kStagingBytes = 16 * 4160;
+
 __device__ __forceinline__ void epi_barrier() {
   asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
 }
