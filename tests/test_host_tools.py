@@ -47,14 +47,27 @@ def _rank_main(rank, world, port, n, f, t, result_path):
     import xgpu_b200 as xg
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
+    import ctypes
     x = oracle.gaussian_input(n, f, t, seed=42)
     f0, f1 = xg.channel_shard(f, world, rank)
     part = oracle.xengine_i64(xg.shard_input(x, n, f, t, f0, f1), n, f1 - f0, t)
+    # The library takes this rank's range as a context of the full band
+    # (XGPUConfig channel_offset / input_nfrequency): without a device the
+    # call gets past argument checking and fails only for want of a GPU.
+    cfg = xg.default_config()
+    cfg.nstation, cfg.ntime, cfg.ntimepipe = n, t, 128
+    cfg.nfrequency, cfg.channel_offset, cfg.input_nfrequency = f1 - f0, f0, f
+    ctx = xg.XGPUContext()
+    rc = xg.lib().xgpuInitEx(ctypes.byref(ctx), 0, ctypes.byref(cfg))   # device 0 on any host
+    accepted = rc in (xg.XGPU_OK, xg.XGPU_CUDA_ERROR)
+    if rc == xg.XGPU_OK:
+        xg.lib().xgpuFree(ctypes.byref(ctx))
     parts = [None] * world
-    dist.all_gather_object(parts, part)
+    dist.all_gather_object(parts, (part, accepted))
     if rank == 0:
-        full = xg.merge_triangular(parts)
-        np.save(result_path, np.array([np.array_equal(full, oracle.xengine_i64(x, n, f, t))]))
+        full = xg.merge_triangular([q[0] for q in parts])
+        ok = np.array_equal(full, oracle.xengine_i64(x, n, f, t)) and all(q[1] for q in parts)
+        np.save(result_path, np.array([ok]))
     dist.barrier()
     dist.destroy_process_group()
 

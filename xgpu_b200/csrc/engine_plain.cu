@@ -42,10 +42,11 @@ __device__ __forceinline__ void decode_block(int k, int &rb, int &cb) {
   cb = k - r * (r + 1) / 2;
 }
 
-// Slot of station s (0..31) inside a converted panel: thread column tx reads
-// stations 2tx and 2tx+1, stored at slots tx and 16+tx so that 16 threads
-// read 256 contiguous bytes.
-__device__ __forceinline__ int slot_of(int s) { return (s & 1) * 16 + (s >> 1); }
+// Station (0..31) held in slot q of a converted panel: thread column tx reads
+// stations 2tx and 2tx+1 from slots tx and 16+tx, so that 16 threads read 256
+// contiguous bytes.  The conversions fill slot q from lane q, so a warp's
+// stores are 32 consecutive slots (no bank conflicts).
+__device__ __forceinline__ int station_of_slot(int q) { return q < 16 ? 2 * q : 2 * (q - 16) + 1; }
 
 struct Params {
   CUtensorMap map;  // the input, boxes of 128 bytes x one chunk of samples
@@ -99,7 +100,7 @@ __device__ __forceinline__ int dp4a(int a, int b, int c) {
 // raw [sample][station][4 bytes] -> words [group][slot][4 words of 4 samples]
 __device__ __forceinline__ void to_words(const uint8_t *raw, int4 *words) {
   for (int u = threadIdx.x; u < kGroups * kBlk; u += kThreads) {
-    const int g = u / kBlk, s = u % kBlk;
+    const int g = u / kBlk, q = u % kBlk, s = station_of_slot(q);
     const uint32_t *r = (const uint32_t *)(raw + (4 * g) * kRowBytes) + s;
     const uint32_t w0 = r[0], w1 = r[kRowBytes / 4], w2 = r[2 * kRowBytes / 4],
                    w3 = r[3 * kRowBytes / 4];
@@ -110,7 +111,7 @@ __device__ __forceinline__ void to_words(const uint8_t *raw, int4 *words) {
     o.y = (int)__byte_perm(lo01, lo23, 0x7632);  // X im
     o.z = (int)__byte_perm(hi01, hi23, 0x5410);  // Y re
     o.w = (int)__byte_perm(hi01, hi23, 0x7632);  // Y im
-    words[g * kBlk + slot_of(s)] = o;
+    words[g * kBlk + q] = o;
   }
 }
 
@@ -240,9 +241,9 @@ constexpr int kFloatPanel = kTcF * kBlk;         // float4 entries: [sample][slo
 
 __device__ __forceinline__ void to_floats(const uint8_t *raw, float4 *fl) {
   for (int u = threadIdx.x; u < kTcF * kBlk; u += kThreads) {
-    const int t = u / kBlk, s = u % kBlk;
+    const int t = u / kBlk, q = u % kBlk, s = station_of_slot(q);
     const char4 b = *(const char4 *)(raw + t * kRowBytes + s * 4);
-    fl[t * kBlk + slot_of(s)] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
+    fl[t * kBlk + q] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
   }
 }
 
