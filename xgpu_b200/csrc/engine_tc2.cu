@@ -25,10 +25,11 @@
 // may run beside the previous one), and its epilogue has two schedules, joint
 // and split per warp, chosen by the length of the launch's items.
 // A second instantiation (kPacked) reads packed 4+4-bit input: each CTA's
-// producer loads the packed bytes into the upper halves of its operand boxes,
-// five converter warps (one per pipeline slot) expand them in place, scaled by
-// 16, and report each stage on the leader's "full" barrier; the drain divides
-// the sums by 256.
+// producer loads its packed boxes with TMA into a ring of packed slots, four
+// converter warps expand every stage from there into an operand stage (the
+// ring of operand stages is shorter, so that both rings fit), scaled by 16,
+// and report it on the leader's "full" barrier; the drain divides the sums
+// by 256.
 #include <cudaTypedefs.h>
 #include <string.h>
 
