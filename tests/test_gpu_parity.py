@@ -298,6 +298,28 @@ def test_caller_buffers_registered_and_offsets(xg, oracle_mod):
         assert not ctx.internal
 
 
+def test_library_buffers_kept_when_set_again(xg, oracle_mod):
+    """xgpuSetHostInputBuffer / xgpuSetHostOutputBuffer called again with the
+    buffers the library allocated (array_h and matrix_h unchanged) keep them:
+    the pointers stay valid, hold what the caller wrote, and the call after
+    them is exact.  (Taken literally, the reference's steps would free the
+    buffer and then register the freed pointer.)"""
+    n, f, t = 32, 2, 128
+    x = oracle_mod.gaussian_input(n, f, t, seed=8)
+    exact = oracle_mod.xengine_i64(x, n, f, t).astype(np.int32)
+    with xg.Correlator(n, f, t, ntimepipe=128, order="tri") as c:
+        c.set_input(x)
+        a, m = c.ctx.array_h, c.ctx.matrix_h
+        L = xg.lib()
+        for _ in range(2):
+            assert L.xgpuSetHostInputBuffer(ctypes.byref(c.ctx)) == 0
+            assert L.xgpuSetHostOutputBuffer(ctypes.byref(c.ctx)) == 0
+        assert (c.ctx.array_h, c.ctx.matrix_h) == (a, m)
+        assert np.array_equal(c.input_view()[: x.size], x)
+        c.run(xg.SYNCOP_DUMP)
+        assert np.array_equal(c.output_view()[: exact.size], exact)
+
+
 def test_reference_api_default_context(xg, oracle_mod):
     """The unmodified xGPU calling sequence (cuda_correlator.c:145-253) at the
     default sizes: xgpuInit with library-allocated buffers, xgpuCudaXengine

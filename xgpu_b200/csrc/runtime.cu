@@ -763,6 +763,14 @@ int xgpuSetHostInputBuffer(XGPUContext *context) {
   if (!in) return XGPU_NOT_INITIALIZED;
   XGPU_CHECK(cudaSetDevice(in->device));
   XGPU_CHECK(cudaStreamSynchronize(in->s_copy));
+  // Called again with the buffer this library allocated: keep it (freeing it
+  // and then registering the freed pointer as a caller's buffer, which is
+  // what taking the steps below in order would do, is undefined).
+  if (in->free_array_h && context->array_h == in->free_array_h) {
+    in->array_h_set = true;
+    context->input_offset = 0;
+    return XGPU_OK;
+  }
   if (in->free_array_h) {
     cudaFreeHost(in->free_array_h);
     in->free_array_h = nullptr;
@@ -794,6 +802,12 @@ int xgpuSetHostOutputBuffer(XGPUContext *context) {
   if (!in) return XGPU_NOT_INITIALIZED;
   XGPU_CHECK(cudaSetDevice(in->device));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
+  // As for the input buffer: the library's own buffer, passed again, stays.
+  if (in->free_matrix_h && context->matrix_h == in->free_matrix_h) {
+    in->matrix_h_set = true;
+    context->output_offset = 0;
+    return XGPU_OK;
+  }
   if (in->free_matrix_h) {
     cudaFreeHost(in->free_matrix_h);
     in->free_matrix_h = nullptr;
@@ -978,8 +992,11 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
     rot = nullptr;
     nrot = 1;
   }
-  if (rot) XGPU_CHECK(launch_generate(rot, nrot * slot_bytes, 0, 12345, 16.0, in->s_comp));
-  else XGPU_CHECK(launch_generate(tune_in, call_bytes, 0, 12345, 16.0, in->s_comp));
+  if ((rot ? launch_generate(rot, nrot * slot_bytes, 0, 12345, 16.0, in->s_comp)
+           : launch_generate(tune_in, call_bytes, 0, 12345, 16.0, in->s_comp)) != cudaSuccess) {
+    if (rot) cudaFree(rot);
+    return XGPU_CUDA_ERROR;
+  }
   void *scratch = nullptr;
   if (cudaMalloc(&scratch, (size_t)s.state_elems * 8) != cudaSuccess) {
     cudaGetLastError();
