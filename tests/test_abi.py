@@ -256,3 +256,26 @@ def test_static_entry_point_rejects_before_any_device_call(xg, change):
     rc = xg.lib().xgpuCorrelateStatic(ctypes.c_void_p(1 << 20), ctypes.c_void_p(1 << 21),
                                       ctypes.byref(cfg), 0, None)
     assert rc == xg.XGPU_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("change", [
+    {"ntime": 2**31 - 128},      # past the planner's int stage count
+    {"nfrequency": 70000},       # past xgpuInitEx's channel range
+    {"nstation": 8208},          # past the station limit
+    {"ntime": 1000},             # not a multiple of 16
+    {"nstation": 40},            # not a multiple of 16
+])
+def test_batch_job_sizes_rejected_before_any_device_call(xg, change):
+    """xgpuBatchCreate applies xgpuInitEx's size checks to every job before
+    touching a device (the buffer addresses below are never dereferenced)."""
+    jobs = (xg.XGPUBatchJob * 2)()
+    for q in range(2):
+        jobs[q].device_input = 1 << 20
+        jobs[q].device_state = 1 << 21
+        jobs[q].nstation, jobs[q].nfrequency, jobs[q].ntime = 64, 2, 256
+    for k, v in change.items():
+        setattr(jobs[1], k, v)
+    b = ctypes.c_void_p()
+    rc = xg.lib().xgpuBatchCreate(ctypes.byref(b), jobs, 2, 0, None, 0)
+    assert rc == xg.XGPU_INVALID_ARGUMENT
+    assert not b.value

@@ -245,9 +245,10 @@ int xgpuBatchCreate(XGPUBatch *out, const XGPUBatchJob *jobs, int njobs, int dev
     c.ntime = j.ntime;
     c.ntimepipe = 16;
     c.matrix_order = TRIANGULAR_ORDER;
+    // xgpuInitEx's ranges for each job (sample and channel counts included:
+    // the planner counts stages and items in int)
     if (!j.device_input || !j.device_state || ((uintptr_t)j.device_input & 15) ||
-        ((uintptr_t)j.device_state & 15) || j.nstation < 16 || j.nstation % 16 ||
-        j.nstation > 8192 || j.nfrequency < 1 || j.ntime < 16 || j.ntime % 16) {
+        ((uintptr_t)j.device_state & 15) || !validate_config(c)) {
       delete b;
       return XGPU_INVALID_ARGUMENT;
     }

@@ -201,7 +201,8 @@ extern "C" int xgpuServeRun(const XGPUServeJob *jobs, int njobs, const XGPUServe
   for (int q = 0; q < njobs; ++q) {
     const XGPUServeJob &j = jobs[q];
     if (j.nstation < 16 || j.nstation % 16 || j.nstation > 8192 || j.nfrequency < 1 ||
-        j.ntime < 16 || j.ntime % 16 || j.ntime > kSegment || j.nblocks < 1 || j.arrival_s < 0 ||
+        j.nfrequency > 65535 || j.ntime < 16 || j.ntime % 16 || j.ntime > kSegment ||
+        j.nblocks < 1 || j.arrival_s < 0 ||
         !(j.sigma > 0) ||
         (q > 0 && j.arrival_s < jobs[q - 1].arrival_s))
       return XGPU_INVALID_ARGUMENT;
