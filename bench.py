@@ -126,7 +126,7 @@ def dist_setup(args):
         import torch.distributed as dist
         from datetime import timedelta
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+        dist.init_process_group("nccl", timeout=timedelta(seconds=180),
                                 device_id=torch.device("cuda", local))
     return world, rank, local
 
@@ -599,7 +599,8 @@ def run_reference(args, world, rank):
         "value": v, "ms_per_step": ms, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
         "data": "synthetic: seeded Gaussian int8, sigma 16",
         "config": {"workload": f"xgpuOmpXengine NSTATION={N} NPOL=2 NFREQUENCY={F} NTIME={T}, "
-                               "one call per step", "nstation": N, "nfrequency": F, "ntime": T},
+                               "one call per step", "nstation": N, "npol": 2, "nfrequency": F,
+                   "ntime": T, "parallelism": "host cores of rank 0 (OpenMP)"},
         "cpu_baseline": {"value": v, "unit": "TOPS", "cores": os.cpu_count(), "kind": "reference",
                          "cpu_model": cpu_model(),
                          "sample": f"{args.steps} calls of the reference xgpuOmpXengine (DP4A "
@@ -627,10 +628,13 @@ def main():
                          "behind the arrivals, so its latency grows with this)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    world, rank, local = dist_setup(args)
     if args.impl == "reference":
-        run_reference(args, world, rank)
+        # CPU only: rank 0 times the reference, the other ranks exit at once;
+        # no process group is needed
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")),
+                      int(os.environ.get("RANK", "0")))
         return
+    world, rank, local = dist_setup(args)
 
     import torch
     import oracle
@@ -763,7 +767,8 @@ def main():
                              "time includes filling and draining the chain of overlapping "
                              "launches (about 35 us per run), so short runs read lower"},
         "e2e": e2e_v, "gpu_launches": args.steps, "roofline": roof,
-        "cpu_baseline": cpu_baseline(), "clocks": clk, "detail": detail,
+        # the host-core baseline is timed at N=1 only
+        "cpu_baseline": cpu_baseline() if world == 1 else None, "clocks": clk, "detail": detail,
     }
     print(json.dumps(line))
     barrier(world)
