@@ -163,3 +163,40 @@ def test_fp32_engine_past_2_24_equals_reference_float_engine(xg, oracle_mod, cal
     assert np.abs(exact).max() > 2 ** 26          # far past exact float integers
     assert not np.array_equal(ref.astype(np.float64), exact)   # the reference rounds here
     assert np.array_equal(got, ref)                # max relative error 0 (tolerance 1e-6)
+
+
+# The largest station counts xgpuInitEx accepts (up to 8192): at N=8192 a
+# channel has 32768 Gram rows, 8256 CTA-pair tile pairs (32896 single-CTA
+# ones, and as many 32x32-station blocks for the plain engine), and its
+# int64 buffer holds 268 million words, so row offsets pass 2^28.  One
+# channel and a few stages keep the oracle in seconds.
+@pytest.mark.parametrize("n", [2048, 4096, 8192])
+@pytest.mark.parametrize("tune", [(1, 0, 1), (1, 0, 0)], ids=["pair", "single"])
+def test_tensor_kernels_at_the_largest_n(xg, oracle_mod, n, tune):
+    f, t = 1, 144    # a partial second stage
+    x = oracle_mod.gaussian_input(n, f, t, seed=n + tune[2], sigma=30.0)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    with xg.Correlator(n, f, t, ntimepipe=16, engine="tensor") as c:
+        c.tune(*tune)
+        c.set_input(x)
+        c.run(xg.SYNCOP_SYNC_COMPUTE)     # stores into the cleared buffer
+        c.set_input(x)
+        c.run(xg.SYNCOP_DUMP)             # adds
+        assert np.array_equal(c.dump_int64(), 2 * exact)
+        got = c.output_view()[: c.info.matLength * 2]
+        assert np.array_equal(got, (2 * exact).astype(np.int32))
+
+
+@pytest.mark.parametrize("n,compute", [(8192, "int8"), (2048, "fp32")])
+def test_plain_engines_at_the_largest_n(xg, oracle_mod, n, compute):
+    t = 64
+    x = oracle_mod.gaussian_input(n, 1, t, seed=n + 1, sigma=20.0)
+    exact = oracle_mod.xengine_i64(x, n, 1, t)
+    output = "int32" if compute == "int8" else "float32"
+    with xg.Correlator(n, 1, t, ntimepipe=16, engine="plain", compute=compute,
+                       output=output) as c:
+        c.set_input(x)
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2]
+        # int8 sums are exact; FP32 sums of 64 samples stay below 2^24, so exact too
+        assert np.array_equal(got, exact.astype(got.dtype))
