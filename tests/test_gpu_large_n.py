@@ -200,3 +200,25 @@ def test_plain_engines_at_the_largest_n(xg, oracle_mod, n, compute):
         got = c.output_view()[: c.info.matLength * 2]
         # int8 sums are exact; FP32 sums of 64 samples stay below 2^24, so exact too
         assert np.array_equal(got, exact.astype(got.dtype))
+
+
+# The largest channel count xgpuInitEx accepts, 65535: the plain engines
+# launch one grid row per channel (gridDim.y at its limit), the tensor-core
+# kernels count 65535 channels' tiles as work items.
+@pytest.mark.parametrize("engine,compute,tune", [
+    ("tensor", "int8", (1, 0, 1)), ("tensor", "int8", (1, 0, 0)),
+    ("plain", "int8", None), ("plain", "fp32", None)],
+    ids=["pair", "single", "dp4a", "fp32"])
+def test_the_largest_channel_count(xg, oracle_mod, engine, compute, tune):
+    n, f, t = 16, 65535, 32
+    x = oracle_mod.gaussian_input(n, f, t, seed=5, sigma=20.0)
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    output = "int32" if compute == "int8" else "float32"
+    with xg.Correlator(n, f, t, ntimepipe=16, engine=engine, compute=compute,
+                       output=output) as c:
+        if tune:
+            c.tune(*tune)
+        c.set_input(x)
+        c.run(xg.SYNCOP_DUMP)
+        got = c.output_view()[: c.info.matLength * 2]
+        assert np.array_equal(got, exact.astype(got.dtype))
