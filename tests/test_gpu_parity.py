@@ -380,20 +380,23 @@ def test_converted_device_input_on_caller_stream(xg, oracle_mod):
         assert np.array_equal(c.dump_int64(), want)
 
 
-@pytest.mark.parametrize("pair,ksplit", [(0, 1), (1, 1), (0, 3), (2, 1)])
-def test_overlapping_accumulating_calls(xg, oracle_mod, pair, ksplit):
+@pytest.mark.parametrize("engine,pair,ksplit", [("tensor", 0, 1), ("tensor", 1, 1),
+                                                ("tensor", 0, 3), ("tensor", 2, 1),
+                                                ("plain", None, None)])
+def test_overlapping_accumulating_calls(xg, oracle_mod, engine, pair, ksplit):
     """Back-to-back accumulating calls over device input on the context's own
     stream: each launch may start before the previous one has finished (the
-    two only add into the integration).  Sums stay exact, also across a dump
-    in the middle and a clear."""
+    two only add into the integration; the plain dp4a engine's time splits
+    too).  Sums stay exact, also across a dump in the middle and a clear."""
     import torch
     n, f, t = 128, 5, 1024
     xs = [oracle_mod.gaussian_input(n, f, t, seed=90 + q, sigma=30.0) for q in range(5)]
     ds = [torch.from_numpy(x).cuda() for x in xs]
     torch.cuda.synchronize()
     one = sum(oracle_mod.xengine_i64(x, n, f, t) for x in xs)
-    with xg.Correlator(n, f, t, engine="tensor") as c:
-        c.tune(ksplit, 0, pair)
+    with xg.Correlator(n, f, t, engine=engine) as c:
+        if engine == "tensor":
+            c.tune(ksplit, 0, pair)
         for _ in range(3):
             for d in ds:
                 c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
@@ -408,14 +411,15 @@ def test_overlapping_accumulating_calls(xg, oracle_mod, pair, ksplit):
         assert np.array_equal(c.dump_int64(), one + oracle_mod.xengine_i64(xs[0], n, f, t))
 
 
-def test_overlapping_calls_of_several_segments(xg, oracle_mod):
+@pytest.mark.parametrize("engine", ["tensor", "plain"])
+def test_overlapping_calls_of_several_segments(xg, oracle_mod, engine):
     """Calls longer than one launch (several time segments) chained back to back."""
     import torch
     n, f, t = 32, 2, 65536 + 512
     xs = [oracle_mod.gaussian_input(n, f, t, seed=70 + q, sigma=20.0) for q in range(2)]
     ds = [torch.from_numpy(x).cuda() for x in xs]
     torch.cuda.synchronize()
-    with xg.Correlator(n, f, t, ntimepipe=128, engine="tensor") as c:
+    with xg.Correlator(n, f, t, ntimepipe=128, engine=engine) as c:
         for d in ds + ds:
             c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
         got = c.dump_int64()

@@ -59,6 +59,7 @@ struct Params {
   int *err;         // receives kErrTimeoutPanel (may be null)
   int stall;        // test switch: issue no panel loads (the waits on them expire)
   int f0;           // first channel (blockIdx.y counts from it)
+  int overlap;      // dp4a: may run beside the previous (adding) launch of the stream
 };
 
 // Queue the TMA loads of samples [tb, tb+NT) of the row panel (and, off the
@@ -153,6 +154,13 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
     (&i2[0][0][0][0])[a] = 0;
   }
 
+  // Programmatic launch (as the tensor-core kernels): unless this launch only
+  // adds into sums that the previous launch of the stream also only adds
+  // into, nothing below reads or writes global memory before that launch has
+  // finished; an overlapping launch waits for it at the end instead, so it
+  // never completes first.  Either way the next launch may start now.
+  if (!p.overlap) tc::pdl_wait();
+  tc::pdl_trigger();
   const uint32_t bar0 = tc::smem_u32(&bars[0]);
   if (threadIdx.x == 0) {
     asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.map) : "memory");
@@ -172,6 +180,7 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
     const bool got = tc::mbar_wait(bar0 + 8 * buf, (ch >> 1) & 1, nullptr);
     if (__syncthreads_or(!got)) {
       panel_timeout(p, bar0 + 8 * (buf ^ 1), ((ch + 1) >> 1) & 1, ch + 1 < nchunks);
+      if (p.overlap) tc::pdl_wait();
       return;
     }
     to_words(raw[buf][0], words[0]);
@@ -259,6 +268,7 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
     }
     __syncthreads();
   }
+  if (p.overlap) tc::pdl_wait();
 }
 
 // ---------------------------------------------------------------- FP32 ----
@@ -444,12 +454,13 @@ static int plain_params(plain::Params *p, const int8_t *in, const Sizes &s, int 
   p->err = err;
   p->stall = stall;
   p->f0 = f0;
+  p->overlap = 0;
   return 0;
 }
 
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
                               int64_t *state, int overwrite, cudaStream_t st, int *err,
-                              int stall, int f0, int fcount) {
+                              int stall, int f0, int fcount, int overlap) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   const int ks = plain_splits(s, fcount, tcount);
@@ -468,9 +479,20 @@ cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcou
   plain::Params p;
   if (plain_params(&p, in, s, t0, tcount, state, overwrite, per, plain::kTcD, err, stall, f0) != 0)
     return cudaErrorInvalidValue;
-  plain::xengine_dp4a_kernel<<<plain_grid(s, fcount, used), plain::kThreads, plain::kSmemDp4a,
-                               st>>>(p);
-  return cudaGetLastError();
+  p.overlap = (overlap && !overwrite) ? 1 : 0;
+  // Programmatic launch: the grid may start beside the previous kernel's last
+  // CTAs (the kernel waits for it where it must).
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = plain_grid(s, fcount, used);
+  cfg.blockDim = dim3(plain::kThreads);
+  cfg.dynamicSmemBytes = plain::kSmemDp4a;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, plain::xengine_dp4a_kernel, p);
 }
 
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount, float *state,

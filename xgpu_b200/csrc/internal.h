@@ -72,9 +72,11 @@ inline Sizes compact_sizes(Sizes s) {
 // The plain engines load their input panels with TMA; err (may be null)
 // receives kErrTimeoutPanel if a panel never arrives.  stall (a test switch)
 // withholds the loads so that happens.
+// overlap: the launch only adds and follows an adding dp4a launch on the
+// same stream (programmatic launch: it may run beside it).
 cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcount,
                               int64_t *state, int overwrite, cudaStream_t st, int *err = nullptr,
-                              int stall = 0, int f0 = 0, int fcount = -1);
+                              int stall = 0, int f0 = 0, int fcount = -1, int overlap = 0);
 cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcount,
                               float *state, int overwrite, cudaStream_t st, int *err = nullptr,
                               int stall = 0, int f0 = 0, int fcount = -1);

@@ -273,8 +273,11 @@ int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fco
   } else if (in->cfg.engine == XGPU_ENGINE_PLAIN) {
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      XGPU_CHECK(launch_plain_dp4a(x, s, t0, tc, (int64_t *)in->d_state, ow && t0 == 0,
-                                   in->s_comp, in->d_err, in->tune.stall, f0, fcount));
+      const int store = ow && t0 == 0;
+      XGPU_CHECK(launch_plain_dp4a(x, s, t0, tc, (int64_t *)in->d_state, store, in->s_comp,
+                                   in->d_err, in->tune.stall, f0, fcount,
+                                   *tail && !store ? 1 : 0));
+      *tail = !store;   // the next segment follows an adding launch
     }
   } else {
     const CUtensorMap *map = tensor_map(in, x, s, packed);
@@ -352,7 +355,7 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready, bool 
   }
   const int r = launch_engine(in, x, *geom, 0, s.f, &tail, packed);
   if (r != XGPU_OK) return r;
-  if (in->int_state && in->cfg.engine == XGPU_ENGINE_TENSOR) in->adding_tail = tail && conv < 0;
+  if (in->int_state) in->adding_tail = tail && conv < 0;   // tensor or dp4a engine
   in->state_zero = false;
   if (conv >= 0) {
     XGPU_CHECK(cudaEventRecord(in->conv_free[conv], in->s_comp));
