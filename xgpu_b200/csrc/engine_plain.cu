@@ -13,8 +13,10 @@
 //   dp4a: 48 int32 accumulators (re, im1, im2 as in kernel.cuh:464-479,574),
 //         64 dp4a per group of 4 samples.
 // What changes is the data path.  xGPU fetches one sample at a time through
-// textures and swizzled input; here a CTA of 256 threads covers a 32x32
-// station block of one channel, stages 128-byte panels of the natural
+// textures and swizzled input; here a CTA covers a station block of one
+// channel -- dp4a: 32x32 stations, 256 threads; FP32: 16x32, 128 threads, so
+// that its CTAs, which may not split time, balance the SMs -- stages 128-byte
+// panels of the natural
 // [t][f][s][p][c] input into shared memory with TMA (one thread issues each
 // chunk's panels on an mbarrier, double buffered; stations past n and samples
 // past the input are zero-filled), and converts them in shared memory -- to 4-sample
@@ -272,34 +274,88 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
 }
 
 // ---------------------------------------------------------------- FP32 ----
+// The FP32 engine may not split time (its sums keep xGPU's order), so it
+// balances the SMs with smaller blocks instead: 16 x 32 stations (rows x
+// columns) per CTA of 128 threads (8 x 16 threads, 2x2 stations each), five
+// CTAs per SM.  At N=256, F=10 that is 720 CTAs, all resident at once, 4.9
+// per SM (32 x 32-station blocks: 360 CTAs, two or three per SM).
 constexpr int kTcF = 32;                         // samples per chunk
 constexpr int kRawPanelF = kTcF * kRowBytes;     // 4 KiB
+constexpr int kRowsF = 16;                       // stations per row block
+constexpr int kThreadsF = (kRowsF / 2) * (kBlk / 2);   // 128
 constexpr int kFloatPanel = kTcF * kBlk;         // float4 entries: [sample][slot]
+constexpr int kFloatPanelRows = kTcF * kRowsF;   // the row block's 16 stations
+
+// Row block k -> (row block r of 16 stations, column block c of 32), r >= 2c:
+// row blocks 2m and 2m + 1 both have m + 1 column blocks at or left of the
+// diagonal, so blocks m(m+1) .. (m+1)^2 - 1 are row 2m, (m+1)^2 .. (m+1)(m+2) - 1
+// row 2m + 1.
+__device__ __forceinline__ void decode_block_f(int k, int &rb, int &cb) {
+  int m = (int)((sqrtf(4.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
+  while (m * (m + 1) > k) --m;
+  while ((m + 1) * (m + 2) <= k) ++m;
+  if (k < (m + 1) * (m + 1)) {
+    rb = 2 * m;
+    cb = k - m * (m + 1);
+  } else {
+    rb = 2 * m + 1;
+    cb = k - (m + 1) * (m + 1);
+  }
+}
+
+// Station (0..15) in slot q of a converted row panel: thread row ty reads
+// stations 2ty and 2ty+1 from slots ty and 8+ty.
+__device__ __forceinline__ int row_station_of_slot(int q) { return q < 8 ? 2 * q : 2 * (q - 8) + 1; }
 
 __device__ __forceinline__ void to_floats(const uint8_t *raw, float4 *fl) {
-  for (int u = threadIdx.x; u < kTcF * kBlk; u += kThreads) {
+  for (int u = threadIdx.x; u < kTcF * kBlk; u += kThreadsF) {
     const int t = u / kBlk, q = u % kBlk, s = station_of_slot(q);
     const char4 b = *(const char4 *)(raw + t * kRowBytes + s * 4);
     fl[t * kBlk + q] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
   }
 }
 
-// Dynamic shared memory of the FP32 kernel: raw panels [2 buffers][2 panels],
-// floats [2 panels], two mbarriers, and room to align the panels to 128 bytes.
-constexpr int kSmemFp32 = 2 * 2 * kRawPanelF + 2 * kFloatPanel * 16 + 16 + 128;
+// The row panel: the first 16 stations of a 32-station panel.
+__device__ __forceinline__ void to_floats_rows(const uint8_t *raw, float4 *fl) {
+  for (int u = threadIdx.x; u < kTcF * kRowsF; u += kThreadsF) {
+    const int t = u / kRowsF, q = u % kRowsF, s = row_station_of_slot(q);
+    const char4 b = *(const char4 *)(raw + t * kRowBytes + s * 4);
+    fl[t * kRowsF + q] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
+  }
+}
 
-__global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_constant__ Params p) {
+// Dynamic shared memory of the FP32 kernel: raw panels [2 buffers][row,
+// column], the converted row and column panels, two mbarriers, and room to
+// align the panels to 128 bytes.
+constexpr int kSmemFp32 =
+    2 * 2 * kRawPanelF + (kFloatPanelRows + kFloatPanel) * 16 + 16 + 128;
+// five CTAs per SM by shared memory (80 registers a thread would allow six)
+static_assert(5 * (kSmemFp32 + 1024) <= 228 * 1024, "five FP32 CTAs per SM");
+
+// The FP32 kernel's panels of samples [tb, tb + kTcF), completing on bar:
+// 32 stations from station 16 rb (its 16 row stations are the first half;
+// stations past n are zero-filled) and the column block's 32 stations.
+// Called by one thread.
+__device__ __forceinline__ void issue_panels_f(uint8_t (*raw)[kRawPanelF], uint32_t bar,
+                                               const Params &p, int f, int rb, int cb, int tb) {
+  if (p.stall) return;
+  tc::mbar_expect_tx(bar, 2 * kRawPanelF);
+  tc::tma_load_3d(tc::smem_u32(raw[0]), &p.map, bar, rb * kRowsF * 4, f, tb);
+  tc::tma_load_3d(tc::smem_u32(raw[1]), &p.map, bar, cb * kRowBytes, f, tb);
+}
+
+__global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_constant__ Params p) {
   extern __shared__ __align__(128) uint8_t dsm_raw[];
   uint8_t *dsm = (uint8_t *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
   auto raw = (uint8_t(*)[2][kRawPanelF])dsm;
-  auto fl = (float4(*)[kFloatPanel])(dsm + 2 * 2 * kRawPanelF);
-  uint64_t *bars = (uint64_t *)(dsm + 2 * 2 * kRawPanelF + 2 * kFloatPanel * 16);
+  float4 *flr = (float4 *)(dsm + 2 * 2 * kRawPanelF);   // row panel, 16 slots
+  float4 *flc = flr + kFloatPanelRows;                   // column panel, 32 slots
+  uint64_t *bars = (uint64_t *)(flc + kFloatPanel);
 
   const int f = p.f0 + (int)blockIdx.y;
-  int rb, cb;
-  decode_block(blockIdx.x, rb, cb);
-  const bool diag = (rb == cb);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  int rb, cb;   // row block of 16 stations, column block of 32
+  decode_block_f(blockIdx.x, rb, cb);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // ty 0..7
   const int nchunks = (p.tcount + kTcF - 1) / kTcF;
 
   // The accumulators continue the integration buffer's sums (0 after a
@@ -310,7 +366,7 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
   for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
     for (int cs = 0; cs < 2; ++cs) {
-      const int i = rb * kBlk + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
+      const int i = rb * kRowsF + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
       const bool mine = !p.overwrite && i < p.n && j <= i;
       const float4 *src = (const float4 *)(state + ((long long)f * p.nbaseline +
                                                     (long long)i * (i + 1) / 2 + j) * 8);
@@ -330,7 +386,7 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
     tc::mbar_init(bar0, 1);
     tc::mbar_init(bar0 + 8, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    issue_panels<kTcF>(raw[0], bar0, p, f, rb, cb, diag, p.t0);
+    issue_panels_f(raw[0], bar0, p, f, rb, cb, p.t0);
   }
   __syncthreads();
 
@@ -338,25 +394,22 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
     const int buf = ch & 1;
     // Chunk ch+1 goes into the other buffer, free since the end of chunk ch-1.
     if (threadIdx.x == 0 && ch + 1 < nchunks)
-      issue_panels<kTcF>(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, diag,
-                         p.t0 + (ch + 1) * kTcF);
+      issue_panels_f(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, p.t0 + (ch + 1) * kTcF);
     const bool got = tc::mbar_wait(bar0 + 8 * buf, (ch >> 1) & 1, nullptr);
     if (__syncthreads_or(!got)) {
       panel_timeout(p, bar0 + 8 * (buf ^ 1), ((ch + 1) >> 1) & 1, ch + 1 < nchunks);
       return;
     }
-    to_floats(raw[buf][0], fl[0]);
-    if (!diag) to_floats(raw[buf][1], fl[1]);
+    to_floats_rows(raw[buf][0], flr);
+    to_floats(raw[buf][1], flc);
     __syncthreads();
-    const float4 *rw = fl[0];
-    const float4 *cw = diag ? fl[0] : fl[1];
 #pragma unroll 4
     for (int t = 0; t < kTcF; ++t) {
       float4 r[2], c[2];
-      r[0] = rw[t * kBlk + ty];
-      r[1] = rw[t * kBlk + 16 + ty];
-      c[0] = cw[t * kBlk + tx];
-      c[1] = cw[t * kBlk + 16 + tx];
+      r[0] = flr[t * kRowsF + ty];
+      r[1] = flr[t * kRowsF + 8 + ty];
+      c[0] = flc[t * kBlk + tx];
+      c[1] = flc[t * kBlk + 16 + tx];
 #pragma unroll
       for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
@@ -385,7 +438,7 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
   for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
     for (int cs = 0; cs < 2; ++cs) {
-      const int i = rb * kBlk + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
+      const int i = rb * kRowsF + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
       if (i >= p.n || j > i) continue;
       float4 *dst = (float4 *)(state + ((long long)f * p.nbaseline +
                                         (long long)i * (i + 1) / 2 + j) * 8);
@@ -401,6 +454,15 @@ __global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_con
 static dim3 plain_grid(const Sizes &s, int fcount, int ksplit = 1) {
   const int nb = (s.n + plain::kBlk - 1) / plain::kBlk;
   return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)fcount, (unsigned)ksplit);
+}
+
+// FP32 blocks: 16-station row blocks r, 32-station column blocks c <= r / 2
+// (decode_block_f).
+static dim3 plain_grid_f(const Sizes &s, int fcount) {
+  const int nr = (s.n + plain::kRowsF - 1) / plain::kRowsF;
+  const int m = nr / 2;
+  const int blocks = nr % 2 == 0 ? m * (m + 1) : (m + 1) * (m + 1);
+  return dim3((unsigned)blocks, (unsigned)fcount, 1);
 }
 
 // Time splits for the dp4a kernel.  With fewer 32x32-station blocks than two
@@ -506,7 +568,8 @@ cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcou
   if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err, stall,
                    f0) != 0)
     return cudaErrorInvalidValue;
-  plain::xengine_fp32_kernel<<<plain_grid(s, fcount), plain::kThreads, plain::kSmemFp32, st>>>(p);
+  plain::xengine_fp32_kernel<<<plain_grid_f(s, fcount), plain::kThreadsF, plain::kSmemFp32,
+                               st>>>(p);
   return cudaGetLastError();
 }
 
