@@ -13,10 +13,9 @@
 //   dp4a: 48 int32 accumulators (re, im1, im2 as in kernel.cuh:464-479,574),
 //         64 dp4a per group of 4 samples.
 // What changes is the data path.  xGPU fetches one sample at a time through
-// textures and swizzled input; here a CTA covers a station block of one
-// channel -- dp4a: 32x32 stations, 256 threads; FP32: 16x32, 128 threads, so
-// that its CTAs, which may not split time, balance the SMs -- stages 128-byte
-// panels of the natural
+// textures and swizzled input; here a CTA of 128 threads covers a block of
+// 16 x 32 stations of one channel (small CTAs balance the SMs: the FP32
+// engine may not split time), stages 128-byte panels of the natural
 // [t][f][s][p][c] input into shared memory with TMA (one thread issues each
 // chunk's panels on an mbarrier, double buffered; stations past n and samples
 // past the input are zero-filled), and converts them in shared memory -- to 4-sample
@@ -32,16 +31,30 @@
 namespace xgpu {
 namespace plain {
 
-constexpr int kBlk = 32;        // stations per block side
-constexpr int kThreads = 256;   // 16 x 16 threads, 2x2 stations each
+// A CTA covers a block of 16 (rows) x 32 (columns) stations of one channel
+// with 128 threads, 8 x 16, each a 2x2 station tile.  Small CTAs balance the
+// SMs: at N=256, F=10 there are 720 of them, five resident per SM, all at
+// once (32 x 32 blocks of 256 threads gave 360 CTAs, two or three per SM).
+constexpr int kBlk = 32;        // stations per column block
+constexpr int kRows = 16;       // stations per row block
+constexpr int kThreads = (kRows / 2) * (kBlk / 2);   // 128
 constexpr int kRowBytes = kBlk * 4;   // one sample of one panel: 32 stations x 2 pol x re/im
 
+// Block k -> (row block r of 16 stations, column block c of 32), 2c <= r:
+// row blocks 2m and 2m + 1 both have m + 1 column blocks at or left of the
+// diagonal, so blocks m(m+1) .. (m+1)^2 - 1 are row 2m, (m+1)^2 ..
+// (m+1)(m+2) - 1 row 2m + 1.
 __device__ __forceinline__ void decode_block(int k, int &rb, int &cb) {
-  int r = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
-  while (r * (r + 1) / 2 > k) --r;
-  while ((r + 1) * (r + 2) / 2 <= k) ++r;
-  rb = r;
-  cb = k - r * (r + 1) / 2;
+  int m = (int)((sqrtf(4.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
+  while (m * (m + 1) > k) --m;
+  while ((m + 1) * (m + 2) <= k) ++m;
+  if (k < (m + 1) * (m + 1)) {
+    rb = 2 * m;
+    cb = k - m * (m + 1);
+  } else {
+    rb = 2 * m + 1;
+    cb = k - (m + 1) * (m + 1);
+  }
 }
 
 // Station (0..31) held in slot q of a converted panel: thread column tx reads
@@ -49,6 +62,10 @@ __device__ __forceinline__ void decode_block(int k, int &rb, int &cb) {
 // contiguous bytes.  The conversions fill slot q from lane q, so a warp's
 // stores are 32 consecutive slots (no bank conflicts).
 __device__ __forceinline__ int station_of_slot(int q) { return q < 16 ? 2 * q : 2 * (q - 16) + 1; }
+
+// Station (0..15) in slot q of a converted row panel: thread row ty reads
+// stations 2ty and 2ty+1 from slots ty and 8+ty.
+__device__ __forceinline__ int row_station_of_slot(int q) { return q < 8 ? 2 * q : 2 * (q - 8) + 1; }
 
 struct Params {
   CUtensorMap map;  // the input, boxes of 128 bytes x one chunk of samples
@@ -64,17 +81,18 @@ struct Params {
   int overlap;      // dp4a: may run beside the previous (adding) launch of the stream
 };
 
-// Queue the TMA loads of samples [tb, tb+NT) of the row panel (and, off the
-// diagonal, the column panel) into raw[0] / raw[1], completing on bar.
-// Called by one thread.
+// Queue the TMA loads of samples [tb, tb+NT) of the row panel and the column
+// panel into raw[0] / raw[1], completing on bar.  Called by one thread.  The
+// row panel is the 32 stations from station 16 rb (its 16 row stations are
+// the first half; stations past n are zero-filled), the column panel the
+// column block's 32 stations.
 template <int NT>
 __device__ __forceinline__ void issue_panels(uint8_t (*raw)[NT * kRowBytes], uint32_t bar,
-                                             const Params &p, int f, int rb, int cb, bool diag,
-                                             int tb) {
+                                             const Params &p, int f, int rb, int cb, int tb) {
   if (p.stall) return;
-  tc::mbar_expect_tx(bar, (diag ? 1 : 2) * NT * kRowBytes);
-  tc::tma_load_3d(tc::smem_u32(raw[0]), &p.map, bar, rb * kRowBytes, f, tb);
-  if (!diag) tc::tma_load_3d(tc::smem_u32(raw[1]), &p.map, bar, cb * kRowBytes, f, tb);
+  tc::mbar_expect_tx(bar, 2 * NT * kRowBytes);
+  tc::tma_load_3d(tc::smem_u32(raw[0]), &p.map, bar, rb * kRows * 4, f, tb);
+  tc::tma_load_3d(tc::smem_u32(raw[1]), &p.map, bar, cb * kRowBytes, f, tb);
 }
 
 // A panel that never arrived (bounded wait expired): record it and leave
@@ -93,6 +111,7 @@ constexpr int kTcD = 64;                        // samples per chunk
 constexpr int kGroups = kTcD / 4;               // 4-sample groups per chunk
 constexpr int kRawPanel = kTcD * kRowBytes;     // 8 KiB
 constexpr int kWordPanel = kGroups * kBlk * 16; // 8 KiB: [group][slot][Xr,Xi,Yr,Yi]
+constexpr int kWordPanelRows = kGroups * kRows * 16;   // 4 KiB: the row block's 16 stations
 
 __device__ __forceinline__ int dp4a(int a, int b, int c) {
   int d;
@@ -101,9 +120,12 @@ __device__ __forceinline__ int dp4a(int a, int b, int c) {
 }
 
 // raw [sample][station][4 bytes] -> words [group][slot][4 words of 4 samples]
+// for the `slots` stations of a panel (32, or the row panel's first 16).
+template <int kSlots>
 __device__ __forceinline__ void to_words(const uint8_t *raw, int4 *words) {
-  for (int u = threadIdx.x; u < kGroups * kBlk; u += kThreads) {
-    const int g = u / kBlk, q = u % kBlk, s = station_of_slot(q);
+  for (int u = threadIdx.x; u < kGroups * kSlots; u += kThreads) {
+    const int g = u / kSlots, q = u % kSlots;
+    const int s = kSlots == kBlk ? station_of_slot(q) : row_station_of_slot(q);
     const uint32_t *r = (const uint32_t *)(raw + (4 * g) * kRowBytes) + s;
     const uint32_t w0 = r[0], w1 = r[kRowBytes / 4], w2 = r[2 * kRowBytes / 4],
                    w3 = r[3 * kRowBytes / 4];
@@ -114,35 +136,37 @@ __device__ __forceinline__ void to_words(const uint8_t *raw, int4 *words) {
     o.y = (int)__byte_perm(lo01, lo23, 0x7632);  // X im
     o.z = (int)__byte_perm(hi01, hi23, 0x5410);  // Y re
     o.w = (int)__byte_perm(hi01, hi23, 0x7632);  // Y im
-    words[g * kBlk + q] = o;
+    words[g * kSlots + q] = o;
   }
 }
 
-// Epilogue staging (in the panels' memory): 16 block rows of 32 baselines x
+// Epilogue staging (in the panels' memory): 8 block rows of 32 baselines x
 // 4 products x {re, im} int64, thread tx's two baselines (128 bytes) at
 // tx * kEpiSeg in its row, 16 bytes apart from the next thread's, so that the
 // eight lanes of each 16-byte store phase write eight different bank groups.
 constexpr int kEpiSeg = 144;
 constexpr int kEpiRow = 16 * kEpiSeg;
 
-// Dynamic shared memory of the dp4a kernel: raw panels [2 buffers][2 panels],
-// converted words [2 panels], two mbarriers, and room to align the panels to
-// 128 bytes (TMA destinations).
-constexpr int kSmemDp4a = 2 * 2 * kRawPanel + 2 * kWordPanel + 16 + 128;
-static_assert(16 * kEpiRow <= 2 * 2 * kRawPanel + 2 * kWordPanel, "epilogue staging fits the panels");
+// Dynamic shared memory of the dp4a kernel: raw panels [2 buffers][row,
+// column], the converted row and column words, two mbarriers, and room to
+// align the panels to 128 bytes (TMA destinations): 45.2 KB, five CTAs per
+// SM (95 registers a thread).
+constexpr int kSmemDp4a = 2 * 2 * kRawPanel + kWordPanelRows + kWordPanel + 16 + 128;
+static_assert(5 * (kSmemDp4a + 1024) <= 228 * 1024, "five dp4a CTAs per SM");
+static_assert((kRows / 2) * kEpiRow <= 2 * 2 * kRawPanel, "epilogue staging fits the panels");
 
-__global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_constant__ Params p) {
+__global__ void __launch_bounds__(kThreads, 5) xengine_dp4a_kernel(const __grid_constant__ Params p) {
   extern __shared__ __align__(128) uint8_t dsm_raw[];
   uint8_t *dsm = (uint8_t *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
   auto raw = (uint8_t(*)[2][kRawPanel])dsm;
-  auto words = (int4(*)[kWordPanel / 16])(dsm + 2 * 2 * kRawPanel);
-  uint64_t *bars = (uint64_t *)(dsm + 2 * 2 * kRawPanel + 2 * kWordPanel);
+  int4 *wrow = (int4 *)(dsm + 2 * 2 * kRawPanel);   // row words, 16 slots
+  int4 *wcol = wrow + kGroups * kRows;               // column words, 32 slots
+  uint64_t *bars = (uint64_t *)(wcol + kGroups * kBlk);
 
   const int f = p.f0 + (int)blockIdx.y;
-  int rb, cb;
+  int rb, cb;   // row block of 16 stations, column block of 32
   decode_block(blockIdx.x, rb, cb);
-  const bool diag = (rb == cb);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // ty 0..7
   // Time split blockIdx.z covers samples [tbeg, tend) of the call's range.
   const int tbeg = p.t0 + (int)blockIdx.z * p.per;
   const int tend = min(p.t0 + p.tcount, tbeg + p.per);
@@ -169,7 +193,7 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
     tc::mbar_init(bar0, 1);
     tc::mbar_init(bar0 + 8, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    issue_panels<kTcD>(raw[0], bar0, p, f, rb, cb, diag, tbeg);
+    issue_panels<kTcD>(raw[0], bar0, p, f, rb, cb, tbeg);
   }
   __syncthreads();
 
@@ -177,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
     const int buf = ch & 1;
     // Chunk ch+1 goes into the other buffer, free since the end of chunk ch-1.
     if (threadIdx.x == 0 && ch + 1 < nchunks)
-      issue_panels<kTcD>(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, diag,
+      issue_panels<kTcD>(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb,
                          tbeg + (ch + 1) * kTcD);
     const bool got = tc::mbar_wait(bar0 + 8 * buf, (ch >> 1) & 1, nullptr);
     if (__syncthreads_or(!got)) {
@@ -185,18 +209,16 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
       if (p.overlap) tc::pdl_wait();
       return;
     }
-    to_words(raw[buf][0], words[0]);
-    if (!diag) to_words(raw[buf][1], words[1]);
+    to_words<kRows>(raw[buf][0], wrow);
+    to_words<kBlk>(raw[buf][1], wcol);
     __syncthreads();
-    const int4 *rw = words[0];
-    const int4 *cw = diag ? words[0] : words[1];
 #pragma unroll 1
     for (int g = 0; g < kGroups; ++g) {
       int4 r[2], c[2];
-      r[0] = rw[g * kBlk + ty];
-      r[1] = rw[g * kBlk + 16 + ty];
-      c[0] = cw[g * kBlk + tx];
-      c[1] = cw[g * kBlk + 16 + tx];
+      r[0] = wrow[g * kRows + ty];
+      r[1] = wrow[g * kRows + 8 + ty];
+      c[0] = wcol[g * kBlk + tx];
+      c[1] = wcol[g * kBlk + 16 + tx];
       // Four sweeps over the 16 visibilities of the 2x2 tile, so that the two
       // dp4a of one real part are 48 instructions apart, not back to back.
 #pragma unroll
@@ -223,7 +245,8 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
 
   // Sums out, half of the block's rows at a time (rs = 0: even rows, 1: odd
   // rows): the threads stage them in shared memory (the panels are free) in
-  // the buffer's order, and each warp then adds two staged rows with 32
+  // the buffer's order, and each of the four warps then adds two of the eight
+  // staged rows with 32
   // consecutive words per instruction -- 256 contiguous bytes, where adding
   // straight from the threads' 2x2 tiles scatters every instruction over 32
   // lines (measured: the epilogue took 20 of 135 us at N=256, F=10, T=1024).
@@ -248,8 +271,8 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
     __syncthreads();
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int r = warp + 8 * h;              // staged row: station i of the block
-      const int i = rb * kBlk + 2 * r + rs;
+      const int r = warp + 4 * h;              // staged row: station i of the block
+      const int i = rb * kRows + 2 * r + rs;
       if (i < p.n) {
         // the row's baselines (i, cb*32 .. cb*32+31) are 256 consecutive
         // words of the buffer; on the diagonal only columns j <= i count
@@ -274,41 +297,15 @@ __global__ void __launch_bounds__(kThreads, 2) xengine_dp4a_kernel(const __grid_
 }
 
 // ---------------------------------------------------------------- FP32 ----
-// The FP32 engine may not split time (its sums keep xGPU's order), so it
-// balances the SMs with smaller blocks instead: 16 x 32 stations (rows x
-// columns) per CTA of 128 threads (8 x 16 threads, 2x2 stations each), five
-// CTAs per SM.  At N=256, F=10 that is 720 CTAs, all resident at once, 4.9
-// per SM (32 x 32-station blocks: 360 CTAs, two or three per SM).
+// The FP32 engine may not split time (its sums keep xGPU's order); the small
+// blocks balance its SMs.
 constexpr int kTcF = 32;                         // samples per chunk
 constexpr int kRawPanelF = kTcF * kRowBytes;     // 4 KiB
-constexpr int kRowsF = 16;                       // stations per row block
-constexpr int kThreadsF = (kRowsF / 2) * (kBlk / 2);   // 128
 constexpr int kFloatPanel = kTcF * kBlk;         // float4 entries: [sample][slot]
-constexpr int kFloatPanelRows = kTcF * kRowsF;   // the row block's 16 stations
-
-// Row block k -> (row block r of 16 stations, column block c of 32), r >= 2c:
-// row blocks 2m and 2m + 1 both have m + 1 column blocks at or left of the
-// diagonal, so blocks m(m+1) .. (m+1)^2 - 1 are row 2m, (m+1)^2 .. (m+1)(m+2) - 1
-// row 2m + 1.
-__device__ __forceinline__ void decode_block_f(int k, int &rb, int &cb) {
-  int m = (int)((sqrtf(4.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
-  while (m * (m + 1) > k) --m;
-  while ((m + 1) * (m + 2) <= k) ++m;
-  if (k < (m + 1) * (m + 1)) {
-    rb = 2 * m;
-    cb = k - m * (m + 1);
-  } else {
-    rb = 2 * m + 1;
-    cb = k - (m + 1) * (m + 1);
-  }
-}
-
-// Station (0..15) in slot q of a converted row panel: thread row ty reads
-// stations 2ty and 2ty+1 from slots ty and 8+ty.
-__device__ __forceinline__ int row_station_of_slot(int q) { return q < 8 ? 2 * q : 2 * (q - 8) + 1; }
+constexpr int kFloatPanelRows = kTcF * kRows;    // the row block's 16 stations
 
 __device__ __forceinline__ void to_floats(const uint8_t *raw, float4 *fl) {
-  for (int u = threadIdx.x; u < kTcF * kBlk; u += kThreadsF) {
+  for (int u = threadIdx.x; u < kTcF * kBlk; u += kThreads) {
     const int t = u / kBlk, q = u % kBlk, s = station_of_slot(q);
     const char4 b = *(const char4 *)(raw + t * kRowBytes + s * 4);
     fl[t * kBlk + q] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
@@ -317,10 +314,10 @@ __device__ __forceinline__ void to_floats(const uint8_t *raw, float4 *fl) {
 
 // The row panel: the first 16 stations of a 32-station panel.
 __device__ __forceinline__ void to_floats_rows(const uint8_t *raw, float4 *fl) {
-  for (int u = threadIdx.x; u < kTcF * kRowsF; u += kThreadsF) {
-    const int t = u / kRowsF, q = u % kRowsF, s = row_station_of_slot(q);
+  for (int u = threadIdx.x; u < kTcF * kRows; u += kThreads) {
+    const int t = u / kRows, q = u % kRows, s = row_station_of_slot(q);
     const char4 b = *(const char4 *)(raw + t * kRowBytes + s * 4);
-    fl[t * kRowsF + q] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
+    fl[t * kRows + q] = make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w);
   }
 }
 
@@ -332,19 +329,7 @@ constexpr int kSmemFp32 =
 // five CTAs per SM by shared memory (80 registers a thread would allow six)
 static_assert(5 * (kSmemFp32 + 1024) <= 228 * 1024, "five FP32 CTAs per SM");
 
-// The FP32 kernel's panels of samples [tb, tb + kTcF), completing on bar:
-// 32 stations from station 16 rb (its 16 row stations are the first half;
-// stations past n are zero-filled) and the column block's 32 stations.
-// Called by one thread.
-__device__ __forceinline__ void issue_panels_f(uint8_t (*raw)[kRawPanelF], uint32_t bar,
-                                               const Params &p, int f, int rb, int cb, int tb) {
-  if (p.stall) return;
-  tc::mbar_expect_tx(bar, 2 * kRawPanelF);
-  tc::tma_load_3d(tc::smem_u32(raw[0]), &p.map, bar, rb * kRowsF * 4, f, tb);
-  tc::tma_load_3d(tc::smem_u32(raw[1]), &p.map, bar, cb * kRowBytes, f, tb);
-}
-
-__global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_constant__ Params p) {
+__global__ void __launch_bounds__(kThreads) xengine_fp32_kernel(const __grid_constant__ Params p) {
   extern __shared__ __align__(128) uint8_t dsm_raw[];
   uint8_t *dsm = (uint8_t *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
   auto raw = (uint8_t(*)[2][kRawPanelF])dsm;
@@ -354,7 +339,7 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
 
   const int f = p.f0 + (int)blockIdx.y;
   int rb, cb;   // row block of 16 stations, column block of 32
-  decode_block_f(blockIdx.x, rb, cb);
+  decode_block(blockIdx.x, rb, cb);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // ty 0..7
   const int nchunks = (p.tcount + kTcF - 1) / kTcF;
 
@@ -366,7 +351,7 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
   for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
     for (int cs = 0; cs < 2; ++cs) {
-      const int i = rb * kRowsF + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
+      const int i = rb * kRows + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
       const bool mine = !p.overwrite && i < p.n && j <= i;
       const float4 *src = (const float4 *)(state + ((long long)f * p.nbaseline +
                                                     (long long)i * (i + 1) / 2 + j) * 8);
@@ -386,7 +371,7 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
     tc::mbar_init(bar0, 1);
     tc::mbar_init(bar0 + 8, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    issue_panels_f(raw[0], bar0, p, f, rb, cb, p.t0);
+    issue_panels<kTcF>(raw[0], bar0, p, f, rb, cb, p.t0);
   }
   __syncthreads();
 
@@ -394,7 +379,7 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
     const int buf = ch & 1;
     // Chunk ch+1 goes into the other buffer, free since the end of chunk ch-1.
     if (threadIdx.x == 0 && ch + 1 < nchunks)
-      issue_panels_f(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, p.t0 + (ch + 1) * kTcF);
+      issue_panels<kTcF>(raw[buf ^ 1], bar0 + 8 * (buf ^ 1), p, f, rb, cb, p.t0 + (ch + 1) * kTcF);
     const bool got = tc::mbar_wait(bar0 + 8 * buf, (ch >> 1) & 1, nullptr);
     if (__syncthreads_or(!got)) {
       panel_timeout(p, bar0 + 8 * (buf ^ 1), ((ch + 1) >> 1) & 1, ch + 1 < nchunks);
@@ -406,8 +391,8 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
 #pragma unroll 4
     for (int t = 0; t < kTcF; ++t) {
       float4 r[2], c[2];
-      r[0] = flr[t * kRowsF + ty];
-      r[1] = flr[t * kRowsF + 8 + ty];
+      r[0] = flr[t * kRows + ty];
+      r[1] = flr[t * kRows + 8 + ty];
       c[0] = flc[t * kBlk + tx];
       c[1] = flc[t * kBlk + 16 + tx];
 #pragma unroll
@@ -438,7 +423,7 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
   for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
     for (int cs = 0; cs < 2; ++cs) {
-      const int i = rb * kRowsF + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
+      const int i = rb * kRows + 2 * ty + rs, j = cb * kBlk + 2 * tx + cs;
       if (i >= p.n || j > i) continue;
       float4 *dst = (float4 *)(state + ((long long)f * p.nbaseline +
                                         (long long)i * (i + 1) / 2 + j) * 8);
@@ -451,40 +436,34 @@ __global__ void __launch_bounds__(kThreadsF) xengine_fp32_kernel(const __grid_co
 
 }  // namespace plain
 
+// Blocks of 16-station rows r and 32-station columns c <= r / 2
+// (decode_block), per channel, times the time splits.
 static dim3 plain_grid(const Sizes &s, int fcount, int ksplit = 1) {
-  const int nb = (s.n + plain::kBlk - 1) / plain::kBlk;
-  return dim3((unsigned)(nb * (nb + 1) / 2), (unsigned)fcount, (unsigned)ksplit);
-}
-
-// FP32 blocks: 16-station row blocks r, 32-station column blocks c <= r / 2
-// (decode_block_f).
-static dim3 plain_grid_f(const Sizes &s, int fcount) {
-  const int nr = (s.n + plain::kRowsF - 1) / plain::kRowsF;
+  const int nr = (s.n + plain::kRows - 1) / plain::kRows;
   const int m = nr / 2;
   const int blocks = nr % 2 == 0 ? m * (m + 1) : (m + 1) * (m + 1);
-  return dim3((unsigned)blocks, (unsigned)fcount, 1);
+  return dim3((unsigned)blocks, (unsigned)fcount, (unsigned)ksplit);
 }
 
-// Time splits for the dp4a kernel.  With fewer 32x32-station blocks than two
-// waves of resident CTAs (two per SM), SMs idle: at N=256, F=10 the 360 blocks
-// leave the second wave mostly empty, and at N=64 the 30 blocks occupy a fifth
-// of the GPU.  Split each block's samples until there are about two waves,
-// keeping at least 256 samples per split and at most 8 splits (each split adds
-// its 8192 sums per block with int64 atomics).  Measured at F=10, T=1024:
-// N=256 155 -> 137 us (2 splits), N=64 60 -> 27 us (4 splits).
-static int plain_splits(const Sizes &s, int fcount, int tcount) {
-  const int slots = 2 * current_device_sms();
+// Time splits of a dp4a launch: enough CTAs for one wave of resident CTAs
+// (five per SM), or for half of one when the launch may overlap the previous
+// adding launch (whose last CTAs, and the next launch's, fill the rest; each
+// split costs its ramp and its atomics), at least 256 samples per split and
+// at most 8 splits.
+static int plain_splits(const Sizes &s, int fcount, int tcount, bool overlap) {
+  const int slots = 5 * current_device_sms();   // resident dp4a CTAs
   if (!slots) return 1;
   const dim3 g = plain_grid(s, fcount);
   const long long blocks = (long long)g.x * g.y;
-  long long k = (2LL * slots + blocks - 1) / blocks;
+  const long long target = overlap ? slots / 2 : slots;
+  long long k = (target + blocks - 1) / blocks;
   if (k > tcount / 256) k = tcount / 256;
   if (k > 8) k = 8;
   return k < 1 ? 1 : (int)k;
 }
 
-// Both kernels take just over 48 KB of shared memory (the panels plus their
-// mbarriers): allow it once per device.
+// The kernels' dynamic shared memory (45.2 and 41.1 KB), allowed once per
+// device.
 static cudaError_t plain_configure_device() {
   static std::atomic<unsigned long long> done{0};
   int dev = 0;
@@ -525,7 +504,7 @@ cudaError_t launch_plain_dp4a(const int8_t *in, const Sizes &s, int t0, int tcou
                               int stall, int f0, int fcount, int overlap) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
-  const int ks = plain_splits(s, fcount, tcount);
+  const int ks = plain_splits(s, fcount, tcount, overlap && !overwrite);
   // samples per split: a whole number of 64-sample chunks
   int per = (tcount + ks - 1) / ks;
   per = (per + plain::kTcD - 1) / plain::kTcD * plain::kTcD;
@@ -568,7 +547,7 @@ cudaError_t launch_plain_fp32(const int8_t *in, const Sizes &s, int t0, int tcou
   if (plain_params(&p, in, s, t0, tcount, state, overwrite, tcount, plain::kTcF, err, stall,
                    f0) != 0)
     return cudaErrorInvalidValue;
-  plain::xengine_fp32_kernel<<<plain_grid_f(s, fcount), plain::kThreadsF, plain::kSmemFp32,
+  plain::xengine_fp32_kernel<<<plain_grid(s, fcount), plain::kThreads, plain::kSmemFp32,
                                st>>>(p);
   return cudaGetLastError();
 }
