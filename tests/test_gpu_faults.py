@@ -68,3 +68,34 @@ def test_packed_input_pair_kernel_expired_wait_is_reported_and_recoverable(xg, o
         c.run(xg.SYNCOP_DUMP)
         got = c.dump_int64()
     assert np.array_equal(got, oracle_mod.xengine_i64(oracle_mod.unpack4(packed), n, f, t))
+
+
+@pytest.mark.parametrize("engine,pair", [("tensor", 1), ("tensor", 0), ("plain", None)])
+def test_expired_waits_in_a_chain_of_overlapping_calls(xg, oracle_mod, engine, pair):
+    """Device-input calls that overlap (programmatic launches that only add)
+    with their waits expiring: each launch gives up on its own bounded waits,
+    waits for its predecessor and returns, the error is reported at the next
+    synchronising call, and the context then works normally."""
+    import torch
+    n, f, t = 64, 2, 512
+    x = oracle_mod.gaussian_input(n, f, t, seed=8)
+    d = torch.from_numpy(x).cuda()
+    torch.cuda.synchronize()
+    exact = oracle_mod.xengine_i64(x, n, f, t)
+    L = xg.lib()
+    with xg.Correlator(n, f, t, engine=engine) as c:
+        if pair is not None:
+            c.tune(1, 0, pair)
+        c.run_device(d.data_ptr(), xg.SYNCOP_SYNC_COMPUTE)     # a stored call, intact
+        assert L.xgpuInjectTimeout(ctypes.byref(c.ctx), 1) == 0
+        c.run_device(d.data_ptr(), xg.SYNCOP_NONE)             # adding calls, overlapping
+        c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        with pytest.raises(xg.XGPUError) as err:
+            c.run_device(d.data_ptr(), xg.SYNCOP_SYNC_COMPUTE)
+        assert err.value.code == xg.XGPU_CUDA_ERROR
+        assert L.xgpuInjectTimeout(ctypes.byref(c.ctx), 0) == 0
+        c.clear()
+        for _ in range(3):
+            c.run_device(d.data_ptr(), xg.SYNCOP_NONE)
+        got = c.dump_int64()
+    assert np.array_equal(got, 3 * exact)
