@@ -76,6 +76,20 @@ def test_static_at_the_size_limit(xg, oracle_mod):
     assert rc == xg.XGPU_INVALID_ARGUMENT
 
 
+def test_static_with_cta_pairs_at_n512(xg, oracle_mod):
+    """From 384 stations on the static path runs the CTA-pair kernel, as a
+    context does before it is tuned: N=512, F=3 (the largest F the static
+    array takes at that N), T=1152 (a partial stage), checked against the
+    oracle in int64-exact int32 words and against the context path."""
+    import torch
+    n, f, t = 512, 3, 1152
+    x = oracle_mod.gaussian_input(n, f, t, seed=171, sigma=30.0)
+    x_dev = torch.from_numpy(x).cuda()
+    got = static_result(xg, torch, x_dev, n, f, t, "tri", "int32")
+    assert np.array_equal(got, oracle_mod.xengine_i64(x, n, f, t).astype(np.int32))
+    assert np.array_equal(got, context_result(xg, x_dev, n, f, t, "tri", "int32"))
+
+
 def test_static_rejects_sizes_beyond_the_array(xg):
     import torch
     cfg = xg.default_config()

@@ -119,9 +119,14 @@ int correlate_static(const void *device_input, void *device_output, const XGPUCo
   CUtensorMap map;
   if (make_tc_tensor_map(&map, device_input, s) != 0) return XGPU_INVALID_ARGUMENT;
   if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return XGPU_CUDA_ERROR;
+  // The kernel a context starts with (it cannot autotune here: that takes
+  // scratch buffers): CTA pairs from 384 stations on, single CTAs below, one
+  // CTA per SM, no time splits.
+  TcTuning tune;
+  tune.wide = c.nstation >= 384 ? 1 : 0;
   for (int t0 = 0; t0 < s.t; t0 += kSegment) {
     const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-    if (launch_tc(map, s, t0, tc, state, t0 == 0 ? 1 : 0, err, st) != cudaSuccess)
+    if (launch_tc_tuned(map, s, t0, tc, state, t0 == 0 ? 1 : 0, err, st, tune, 0) != cudaSuccess)
       return XGPU_CUDA_ERROR;
   }
   if (launch_format(state, 0, s, (int)c.matrix_order, (int)c.output_type, device_output, st) !=
