@@ -62,6 +62,14 @@ constexpr uint32_t kAccCols = 2 * kHalf;    // 256 columns per accumulator
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kThreads = 192;
 constexpr uint32_t kIdesc = i8_idesc(2 * kHalf, 2 * kHalf);
+// Word buffer (word mode): per channel, per 32 x 32-station block (rb >= cb,
+// index rb(rb+1)/2 + cb) 4096 words, ordered (epilogue warp q: stations 8q ..
+// 8q+7) x (baseline jl of the block's 32) x (station 8q + ilq) x (product).
+constexpr int kWordsWarpBytes = 8 * kStations * 4 * 8;   // 8 KB
+static_assert(4 * kWordsWarpBytes <= kStagingBytes, "word staging fits the staging area");
+__host__ __device__ __forceinline__ long long word_offset(int f, long long nblk, int rb, int cb) {
+  return ((long long)f * nblk + (long long)rb * (rb + 1) / 2 + cb) * 4096;
+}
 // Packed 4+4-bit input (one byte per complex sample, 2n bytes per sample):
 // the producer loads each CTA's packed boxes (64 bytes per sample row: 32
 // stations) with TMA into a ring of kPackedSlots slots of its own, and
@@ -98,6 +106,11 @@ struct Params {
   int stall;           // test switch: issue no loads (the waits on them expire)
   int overlap;         // may run alongside the previous (accumulating) launch of the stream
   int split_epi;       // epilogue schedule: 0 joint, 1 split per warp
+  // Word mode (single-job adding launches, split epilogue): the call's sums
+  // go to this block-major word buffer instead of the int64 buffer
+  // (word_offset); words_nblk = 32-station blocks per channel.
+  uint64_t *words;
+  long long words_nblk;
 };
 
 // A decoded work item, 64 bytes; the leader's scheduler writes it into both
@@ -643,6 +656,47 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
         const int hlast = (2 * t.C + 1 > rb) ? 0 : 1;   // last column block at or below the diagonal
         for (int h = 0; h <= hlast; ++h) {
           const int cb = 2 * t.C + h;
+          if (p.words) {
+            // Word mode: each visibility's sums of this call as one 64-bit
+            // word, im * 2^32 + re, staged as this warp's 8 KB of the block
+            // (32 baselines x its 8 stations x 4 products: 32 consecutive
+            // words per store) and added with one bulk reduce-add.
+            uint32_t v[kHalf / 32][32];
+            tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccCols + h * kHalf),
+                       v);
+            if (h == hlast) {
+              asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+              __syncwarp();
+              if (lane == 0) remote_arrive(peer_addr(tempty0 + 8 * acc, 0));
+            }
+            // lane 0 committed this warp's previous copy: its staging is free
+            // once that copy has read it
+            if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            __syncwarp();
+            uint64_t *wst = (uint64_t *)(sstate + quarter * kWordsWarpBytes);
+#pragma unroll
+            for (int q = 0; q < kHalf / 32; ++q) {
+#pragma unroll
+              for (int jj = 0; jj < 8; ++jj) {
+                const int v0 = (int)v[q][4 * jj], v1 = (int)v[q][4 * jj + 1];
+                const int v2 = (int)v[q][4 * jj + 2], v3 = (int)v[q][4 * jj + 3];
+                const int ra = __shfl_xor_sync(0xffffffffu, c ? v0 : v2, 1);
+                const int rb2 = __shfl_xor_sync(0xffffffffu, c ? v1 : v3, 1);
+                const long long re = unscale<kPacked>(c ? (long long)ra + v3 : (long long)v0 + rb2);
+                const long long im = unscale<kPacked>(c ? (long long)v2 - rb2 : (long long)ra - v1);
+                wst[(q * 8 + jj) * 32 + lane] =
+                    ((unsigned long long)im << 32) + (unsigned long long)re;
+              }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+              uint64_t *dst = p.words + word_offset(t.f, p.words_nblk, rb, cb) + quarter * 1024;
+              bulk_reduce_add(dst, smem_u32(wst), kWordsWarpBytes);
+              asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            }
+            continue;
+          }
           uint8_t *srow = sstate + staging_row(il) + (p1 * 2 + c) * 16;
           int jmax = t.n - cb * kStations;
           if (jmax > kStations) jmax = kStations;
@@ -750,7 +804,53 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
   }
 }
 
+// The fold: one thread per word adds it, split into its int32 parts, to the
+// int64 buffer (rows i < n, columns j <= i; the block's other entries hold
+// nothing) and zeroes it.  Each int64 value has one writer.
+__global__ void fold_words_kernel(uint64_t *words, int64_t *state, int n, long long nbaseline,
+                                  long long nblk, long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long blkg = idx >> 12;
+    const int w = (int)(idx & 4095);
+    const int f = (int)(blkg / nblk);
+    const long long k = blkg - (long long)f * nblk;
+    int rb = (int)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
+    while ((long long)rb * (rb + 1) / 2 > k) --rb;
+    while ((long long)(rb + 1) * (rb + 2) / 2 <= k) ++rb;
+    const int cb = (int)(k - (long long)rb * (rb + 1) / 2);
+    const int q = w >> 10, jl = (w >> 5) & 31, ilq = (w >> 2) & 7, pp = w & 3;
+    const long long i = (long long)rb * kStations + 8 * q + ilq;
+    const long long j = (long long)cb * kStations + jl;
+    const uint64_t word = words[idx];
+    if (word != 0 && i < n && j <= i) {
+      const long long re = (long long)(int)(uint32_t)word;                  // low part, signed
+      const long long im = (long long)(word - (unsigned long long)re) >> 32;  // exact: |re| < 2^31
+      int64_t *d = state + (((long long)f * nbaseline + i * (i + 1) / 2 + j) * 4 + pp) * 2;
+      d[0] += re;
+      d[1] += im;
+    }
+    if (word != 0) words[idx] = 0;
+  }
+}
+
 }  // namespace tc2
+
+long long words_blocks(const Sizes &s) {
+  const long long nb = (s.n + tc2::kStations - 1) / tc2::kStations;
+  return nb * (nb + 1) / 2;
+}
+
+long long words_elems(const Sizes &s) { return (long long)s.f * words_blocks(s) * 4096; }
+
+cudaError_t launch_fold_words(uint64_t *words, int64_t *state, const Sizes &s, cudaStream_t st) {
+  const long long total = words_elems(s);
+  long long b = (total + 255) / 256;
+  if (b > 148LL * 16) b = 148LL * 16;
+  tc2::fold_words_kernel<<<(unsigned)b, 256, 0, st>>>(words, state, s.n, s.nbaseline,
+                                                       words_blocks(s), total);
+  return cudaGetLastError();
+}
 
 cudaError_t tc2_set_smem_attribute() {
   cudaError_t e = cudaFuncSetAttribute(tc2::xengine_tc2_kernel<false>,
@@ -762,7 +862,7 @@ cudaError_t tc2_set_smem_attribute() {
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap,
-                       int f0, int fcount, const void *packed_in) {
+                       int f0, int fcount, const void *packed_in, uint64_t *words) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   const bool packed = packed_in != nullptr;   // `map` describes it (make_packed_map)
@@ -808,7 +908,10 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   p.err = err;
   p.stall = tune.stall;
   p.overlap = (overlap && !overwrite) ? 1 : 0;
-  p.split_epi = per <= tc2::kSplitEpilogueSteps ? 1 : 0;
+  // word mode (adding launches only) uses the split epilogue
+  p.words = overwrite ? nullptr : words;
+  p.words_nblk = words_blocks(s);
+  p.split_epi = (p.words || per <= tc2::kSplitEpilogueSteps) ? 1 : 0;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
   if (clusters > p.total) clusters = p.total;
   if (clusters < 1) clusters = 1;
@@ -847,6 +950,8 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
   p.err = err;
   p.stall = 0;
   p.overlap = 0;
+  p.words = nullptr;
+  p.words_nblk = 0;
   p.split_epi = max_item_steps <= tc2::kSplitEpilogueSteps ? 1 : 0;
   int clusters = (grid > 0 ? grid : sms) / 2;
   if (clusters > total_items) clusters = total_items;

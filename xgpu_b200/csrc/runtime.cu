@@ -86,6 +86,14 @@ struct Internal {
   // of device-resident input here (on s_conv) before converting them.
   void *d_slice = nullptr;
   void *d_state = nullptr;             // integration buffer
+  // Adding launches of the CTA-pair kernel add their sums to this word
+  // buffer (one 64-bit word per visibility, im * 2^32 + re: half the bytes of
+  // the int64 buffer's pairs); a fold adds the words into d_state before it
+  // is read and before more than kWordsMaxSamples samples have gone in.
+  // nullptr: no word buffer (it could not be allocated, or another engine).
+  uint64_t *d_words = nullptr;
+  long long words_samples = 0;         // samples in the words since the last fold
+  bool words_dirty = false;
   void *d_out = nullptr;               // formatted dump
   int *d_err = nullptr;                // device error word
   int *h_err = nullptr;                // pinned copy of it
@@ -202,6 +210,7 @@ int free_device(Internal *in) {
   if (in->caller_ev) cudaEventDestroy(in->caller_ev);
   if (in->d_slice) cudaFree(in->d_slice);
   if (in->d_state) cudaFree(in->d_state);
+  if (in->d_words) cudaFree(in->d_words);
   if (in->d_out) cudaFree(in->d_out);
   if (in->d_err) cudaFree(in->d_err);
   if (in->h_err) cudaFreeHost(in->h_err);
@@ -262,10 +271,24 @@ bool packed_in_kernel(const Internal *in) {
 // first segment stores when the buffer is known to be zero.  x has geometry s
 // (in->szc for the context's compact buffers, in->sz for a full-band device
 // input read in place, x then pointing at the context's first channel).
+// Add the words into the int64 buffer (and zero them), on s_comp after
+// everything queued there: before the buffer is read, and before the words
+// would hold more than kWordsMaxSamples samples.  An ordinary launch: the
+// next engine launch does not overlap it.
+int fold_words(Internal *in) {
+  if (!in->words_dirty) return XGPU_OK;
+  XGPU_CHECK(launch_fold_words(in->d_words, (int64_t *)in->d_state, in->szc, in->s_comp));
+  in->words_dirty = false;
+  in->words_samples = 0;
+  in->adding_tail = false;
+  return XGPU_OK;
+}
+
 // *tail: in, the launch may overlap the adding launch before it; out, the
-// last launch queued only added.
+// last launch queued only added.  allow_words: adding launches of the
+// CTA-pair kernel may add into the word buffer.
 int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fcount, bool *tail,
-                  bool packed = false) {
+                  bool packed = false, bool allow_words = true) {
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
     XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
@@ -288,9 +311,20 @@ int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fco
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
       const int store = ow && t0 == 0;
+      const bool words = allow_words && in->d_words && in->tune.wide && !store;
+      if (words && in->words_samples + tc > kWordsMaxSamples) {
+        const int r = fold_words(in);
+        if (r != XGPU_OK) return r;
+        *tail = false;   // the fold is an ordinary launch
+      }
       XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
                                  in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount,
-                                 packed ? (const void *)x : nullptr));
+                                 packed ? (const void *)x : nullptr,
+                                 words ? in->d_words : nullptr));
+      if (words) {
+        in->words_samples += tc;
+        in->words_dirty = true;
+      }
       *tail = !store;   // the next segment follows an adding launch
     }
   }
@@ -403,6 +437,10 @@ int dump(XGPUContext *ctx, Internal *in) {
   if (!in->matrix_h_set || !ctx->matrix_h) return XGPU_HOST_BUFFER_NOT_SET;
   if (ctx->matrix_len && ctx->output_offset + (size_t)in->sz.mat_length > ctx->matrix_len)
     return XGPU_INVALID_ARGUMENT;
+  {
+    const int r = fold_words(in);
+    if (r != XGPU_OK) return r;
+  }
   if (in->state_zero) {
     XGPU_CHECK(cudaMemsetAsync(in->d_state, 0, (size_t)in->sz.state_elems * (in->int_state ? 8 : 4),
                                in->s_comp));
@@ -477,6 +515,13 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
     }
     bound[++ng] = s.f;
   }
+  // Earlier calls' words go into the int64 buffer first: each group's
+  // results are formatted from it right after the group's own launch, which
+  // adds there directly.
+  {
+    const int r = fold_words(in);
+    if (r != XGPU_OK) return r;
+  }
   // The buffer is free once the engine launch that last read it has finished.
   XGPU_CHECK(cudaStreamWaitEvent(in->s_copy, in->comp_done[b], 0));
   for (int k = 0; k < ng; ++k) {
@@ -495,7 +540,7 @@ int dump_call_grouped(XGPUContext *ctx, Internal *in, int b, int groups) {
     const int f0 = bound[k], fc = bound[k + 1] - bound[k];
     XGPU_CHECK(cudaStreamWaitEvent(in->s_comp, in->group_in[k], 0));
     bool tail = false;
-    int r = launch_engine(in, dst, in->szc, f0, fc, &tail, packed);
+    int r = launch_engine(in, dst, in->szc, f0, fc, &tail, packed, false);
     if (r != XGPU_OK) return r;
     if (direct) {
       XGPU_CHECK(cudaEventRecord(in->group_out[k], in->s_comp));
@@ -724,6 +769,15 @@ int xgpuInitEx(XGPUContext *context, int device_flags, const XGPUConfig *cfg_in)
         cudaEventCreateWithFlags(&in->group_out[k], cudaEventDisableTiming) != cudaSuccess)
       return fail(XGPU_CUDA_ERROR);
   }
+  if (in->int_state && cfg.engine == XGPU_ENGINE_TENSOR) {
+    const size_t wbytes = (size_t)words_elems(in->szc) * 8;
+    if (cudaMalloc(&in->d_words, wbytes) != cudaSuccess) {
+      cudaGetLastError();   // the engine then adds into the int64 buffer directly
+      in->d_words = nullptr;
+    } else if (cudaMemsetAsync(in->d_words, 0, wbytes, in->s_comp) != cudaSuccess) {
+      return fail(XGPU_CUDA_ERROR);
+    }
+  }
   if (cudaMemsetAsync(in->d_err, 0, sizeof(int), in->s_comp) != cudaSuccess ||
       cudaMemsetAsync(in->d_state, 0, state_bytes, in->s_comp) != cudaSuccess ||
       cudaStreamSynchronize(in->s_comp) != cudaSuccess)
@@ -756,7 +810,14 @@ int xgpuClearDeviceIntegrationBuffer(XGPUContext *context) {
   Internal *in = get(context);
   if (!in) return XGPU_NOT_INITIALIZED;
   XGPU_CHECK(cudaSetDevice(in->device));
-  // Ordered after queued engine launches; the next launch overwrites.
+  // Ordered after queued engine launches; the next launch overwrites.  Words
+  // not yet folded belong to the integration being discarded.
+  if (in->words_dirty) {
+    XGPU_CHECK(cudaMemsetAsync(in->d_words, 0, (size_t)words_elems(in->szc) * 8, in->s_comp));
+    in->words_dirty = false;
+    in->words_samples = 0;
+  }
+  in->adding_tail = false;
   in->state_zero = true;
   return XGPU_OK;
 }
@@ -926,6 +987,10 @@ int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_o
   XGPU_CHECK(cudaSetDevice(in->device));
   in->adding_tail = false;
   const size_t bytes = (size_t)in->sz.state_elems * 8;
+  {
+    const int r = fold_words(in);
+    if (r != XGPU_OK) return r;
+  }
   if (in->state_zero) {
     XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
     memset(host_out, 0, bytes);
@@ -1000,8 +1065,13 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
     if (rot) cudaFree(rot);
     return XGPU_CUDA_ERROR;
   }
+  // Scratch integration buffer; CTA-pair candidates add into it as words
+  // when the context has a word buffer (as their calls will).
   void *scratch = nullptr;
-  if (cudaMalloc(&scratch, (size_t)s.state_elems * 8) != cudaSuccess) {
+  size_t scratch_bytes = (size_t)s.state_elems * 8;
+  if (in->d_words && (size_t)words_elems(s) * 8 > scratch_bytes)
+    scratch_bytes = (size_t)words_elems(s) * 8;
+  if (cudaMalloc(&scratch, scratch_bytes) != cudaSuccess) {
     cudaGetLastError();
     if (rot) cudaFree(rot);
     return XGPU_OUT_OF_MEMORY;
@@ -1063,8 +1133,9 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
       next_map = (next_map + 1) % nrot;
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
+        uint64_t *words = (in->d_words && t.wide) ? (uint64_t *)scratch : nullptr;
         if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t,
-                            overlap) != cudaSuccess)
+                            overlap, 0, -1, nullptr, words) != cudaSuccess)
           return false;
         overlap = chain;
       }
