@@ -836,6 +836,16 @@ __global__ void fold_words_kernel(uint64_t *words, int64_t *state, int n, long l
 
 }  // namespace tc2
 
+// Items of at most kSplitEpilogueSteps stages drain with the split epilogue,
+// where the reduce-adds outlast the MMAs: those add words.  Longer items keep
+// the joint epilogue and add into the int64 buffer.
+bool tc2_uses_words(int tcount, const TcTuning &tune) {
+  const int total_steps = (tcount + tc2::kKt - 1) / tc2::kKt;
+  int ksplit = tune.ksplit < 1 ? 1 : (tune.ksplit > total_steps ? total_steps : tune.ksplit);
+  const int per = (total_steps + ksplit - 1) / ksplit;
+  return per <= tc2::kSplitEpilogueSteps;
+}
+
 long long words_blocks(const Sizes &s) {
   const long long nb = (s.n + tc2::kStations - 1) / tc2::kStations;
   return nb * (nb + 1) / 2;
@@ -908,8 +918,8 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   p.err = err;
   p.stall = tune.stall;
   p.overlap = (overlap && !overwrite) ? 1 : 0;
-  // word mode (adding launches only) uses the split epilogue
-  p.words = overwrite ? nullptr : words;
+  // word mode: adding launches of short items (tc2_uses_words), split epilogue
+  p.words = (!overwrite && per <= tc2::kSplitEpilogueSteps) ? words : nullptr;
   p.words_nblk = words_blocks(s);
   p.split_epi = (p.words || per <= tc2::kSplitEpilogueSteps) ? 1 : 0;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;

@@ -113,6 +113,9 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
 // words into the int64 buffer (triangular order) and zeroes them.  Exact while
 // every sum in the words is below 2^31 in magnitude (65535 samples).
 long long words_blocks(const Sizes &s);   // 32-station blocks per channel
+// Whether an adding CTA-pair launch of tcount samples with `tune` adds words
+// (its items are short enough for the split epilogue).
+bool tc2_uses_words(int tcount, const TcTuning &tune);
 long long words_elems(const Sizes &s);
 cudaError_t launch_fold_words(uint64_t *words, int64_t *state, const Sizes &s, cudaStream_t st);
 constexpr int kWordsMaxSamples = 65535;

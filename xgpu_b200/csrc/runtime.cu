@@ -311,7 +311,8 @@ int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fco
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
       const int store = ow && t0 == 0;
-      const bool words = allow_words && in->d_words && in->tune.wide && !store;
+      const bool words = allow_words && in->d_words && in->tune.wide && !store &&
+                         tc2_uses_words(tc, in->tune);
       if (words && in->words_samples + tc > kWordsMaxSamples) {
         const int r = fold_words(in);
         if (r != XGPU_OK) return r;
@@ -1133,7 +1134,8 @@ int xgpuTune(XGPUContext *context, int ksplit, int grid, int pair) {
       next_map = (next_map + 1) % nrot;
       for (int t0 = 0; t0 < s.t; t0 += kSegment) {
         const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-        uint64_t *words = (in->d_words && t.wide) ? (uint64_t *)scratch : nullptr;
+        uint64_t *words =
+            (in->d_words && t.wide && tc2_uses_words(tc, t)) ? (uint64_t *)scratch : nullptr;
         if (launch_tc_tuned(map, s, t0, tc, (int64_t *)scratch, 0, in->d_err, in->s_comp, t,
                             overlap, 0, -1, nullptr, words) != cudaSuccess)
           return false;
