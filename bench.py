@@ -148,6 +148,28 @@ def max_over_ranks(world, value):
 
 
 TUNING = {}   # (engine, n, f, t) -> the tensor engine's autotuned setting
+FOLDS = {}    # (engine, n, f, t) -> word-buffer folds inside the timed region
+WORD_MAX_SAMPLES = 65535
+
+
+def word_folds(tuning, t, warmup, steps):
+    """Launches of the library's fold kernel inside a timed run of `steps`
+    calls after `warmup` (the first warm-up call stores): CTA-pair launches
+    whose items take at most 8 stages of 128 samples add into a word buffer,
+    folded before it would pass 65535 samples and once at the closing flush."""
+    if not tuning or not tuning["pair"]:
+        return 0
+    stages = -(-t // 128)
+    ksplit = max(1, min(tuning["ksplit"], stages))
+    if -(-stages // ksplit) > 8:
+        return 0
+    samples, folds = 0, 0
+    for k in range(1, warmup + steps):
+        if samples + t > WORD_MAX_SAMPLES:
+            folds += k >= warmup
+            samples = 0
+        samples += t
+    return folds + (samples > 0)
 
 
 def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, seed=1,
@@ -179,11 +201,16 @@ def device_engine_ms(xg, torch, engine, compute, n, f, t, steps, warmup, world, 
     e0.record(stream)
     for k in range(steps):
         c.run_device(bufs[k % nbuf].data_ptr(), xg.SYNCOP_NONE)
+    # The integration is complete on the device when the region ends: sums
+    # that the CTA-pair kernel keeps in its short-term word buffer are added
+    # into the int64 buffer inside the timed region.
+    c.flush()
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     ms = e0.elapsed_time(e1) / steps
     TUNING[(engine, n, f, t)] = c.tuning() if engine == "tensor" else None
+    FOLDS[(engine, n, f, t)] = word_folds(TUNING[(engine, n, f, t)], t, warmup, steps)
     c.close()
     del bufs
     torch.cuda.empty_cache()
@@ -763,10 +790,13 @@ def main():
                    "tuning": TUNING.get(("tensor", N, F, T)),
                    "launches": "programmatic (PDL): each accumulating call may start while the "
                                "previous call's launch finishes; ms_per_step is the spacing",
-                   "timing": "CUDA events on the context's stream around the K calls; the "
-                             "time includes filling and draining the chain of overlapping "
-                             "launches (about 35 us per run), so short runs read lower"},
-        "e2e": e2e_v, "gpu_launches": args.steps, "roofline": roof,
+                   "timing": "CUDA events on the context's stream around the K calls and "
+                             "the closing xgpuFlushIntegrationBuffer (the word buffer's "
+                             "fold into the int64 buffer); the time includes filling and "
+                             "draining the chain of overlapping launches (about 35 us per "
+                             "run), so short runs read lower"},
+        "e2e": e2e_v, "gpu_launches": args.steps + FOLDS.get(("tensor", N, F, T), 0),
+        "roofline": roof,
         # the host-core baseline is timed at N=1 only
         "cpu_baseline": cpu_baseline() if world == 1 else None, "clocks": clk, "detail": detail,
     }

@@ -265,6 +265,14 @@ int xgpuCudaXengineDevice(XGPUContext *context, const void *device_input, int sy
  * Integer engines only. */
 int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_out);
 
+/* Complete the integration on the device without reading it.  Accumulating
+ * calls of the tensor engine may keep their sums in a short-term buffer that
+ * is added into the integration buffer before every dump; this queues that
+ * addition on the compute stream now (no host wait), so that work timed or
+ * ordered on that stream up to this point includes it.  A no-op when nothing
+ * is pending, and for the other engines. */
+int xgpuFlushIntegrationBuffer(XGPUContext *context);
+
 /* ---- Test and benchmark hooks (not part of xGPU's API; a correlator
  * pipeline needs none of the three below) ---------------------------------- */
 

@@ -169,6 +169,7 @@ def test_errors_before_init(xg):
     assert L.xgpuSetHostOutputBuffer(p) == xg.XGPU_NOT_INITIALIZED
     assert L.xgpuDumpDeviceIntegrationBuffer(p) == xg.XGPU_NOT_INITIALIZED
     assert L.xgpuCudaXengineDevice(p, None, 0) == xg.XGPU_NOT_INITIALIZED
+    assert L.xgpuFlushIntegrationBuffer(p) == xg.XGPU_NOT_INITIALIZED
     L.xgpuFree(p)
     L.xgpuFree(p)  # idempotent, as cuda_xengine.cu:537
 

@@ -146,6 +146,7 @@ _PROTOTYPES = [
                                              ctypes.c_int]),
     ("xgpuDumpDeviceIntegrationBufferInt64", ctypes.c_int, [ctypes.POINTER(XGPUContext),
                                                             ctypes.c_void_p]),
+    ("xgpuFlushIntegrationBuffer", ctypes.c_int, [ctypes.POINTER(XGPUContext)]),
     ("xgpuGenerateDevice", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
                                           ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int]),
     ("xgpuMeasureCorePeak", ctypes.c_int, [ctypes.c_int, ctypes.c_int,
@@ -306,6 +307,12 @@ class Correlator:
         check("xgpuDumpDeviceIntegrationBufferInt64",
               lib().xgpuDumpDeviceIntegrationBufferInt64(ctypes.byref(self.ctx), out.ctypes.data))
         return out
+
+    def flush(self):
+        """Queue the addition of pending short-term sums into the integration
+        buffer on the compute stream (no host wait)."""
+        return check("xgpuFlushIntegrationBuffer",
+                     lib().xgpuFlushIntegrationBuffer(ctypes.byref(self.ctx)))
 
     def clear(self):
         return check("xgpuClearDeviceIntegrationBuffer",

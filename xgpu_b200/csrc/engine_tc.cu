@@ -541,12 +541,12 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
                             const TcTuning &tune, int overlap, int f0, int fcount,
-                            const void *packed_in, uint64_t *words) {
+                            const void *packed_in, uint64_t *words, int words_store) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   if (tune.wide)
     return launch_tc2(map, s, t0, tcount, state, overwrite, err, st, tune, overlap, f0, fcount,
-                      packed_in, words);
+                      packed_in, words, words_store);
   if (packed_in) return cudaErrorInvalidValue;   // only the CTA-pair kernel expands packed input
   const int sms = current_device_sms();
   if (!sms) return cudaErrorInvalidDevice;

@@ -106,11 +106,14 @@ struct Params {
   int stall;           // test switch: issue no loads (the waits on them expire)
   int overlap;         // may run alongside the previous (accumulating) launch of the stream
   int split_epi;       // epilogue schedule: 0 joint, 1 split per warp
-  // Word mode (single-job adding launches, split epilogue): the call's sums
-  // go to this block-major word buffer instead of the int64 buffer
-  // (word_offset); words_nblk = 32-station blocks per channel.
+  // Word mode (single-job launches, split epilogue): the call's sums go to
+  // this block-major word buffer instead of the int64 buffer (word_offset);
+  // words_nblk = 32-station blocks per channel.  words_store: the launch
+  // stores its words (one item per tile: each word has one writer) instead of
+  // adding them.
   uint64_t *words;
   long long words_nblk;
+  int words_store;
 };
 
 // A decoded work item, 64 bytes; the leader's scheduler writes it into both
@@ -669,6 +672,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
               __syncwarp();
               if (lane == 0) remote_arrive(peer_addr(tempty0 + 8 * acc, 0));
             }
+            // The second CTA of a pair tile that ends past the last station
+            // holds a block with no stations: it has no place in the words
+            // (its offset would be another block's).
+            if (rb * kStations >= t.n) continue;
             // lane 0 committed this warp's previous copy: its staging is free
             // once that copy has read it
             if (copier) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -692,7 +699,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
             __syncwarp();
             if (lane == 0) {
               uint64_t *dst = p.words + word_offset(t.f, p.words_nblk, rb, cb) + quarter * 1024;
-              bulk_reduce_add(dst, smem_u32(wst), kWordsWarpBytes);
+              if (p.words_store) bulk_store(dst, smem_u32(wst), kWordsWarpBytes);
+              else bulk_reduce_add(dst, smem_u32(wst), kWordsWarpBytes);
               asm volatile("cp.async.bulk.commit_group;" ::: "memory");
             }
             continue;
@@ -804,33 +812,70 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPacked ? kThreadsPa
   }
 }
 
-// The fold: one thread per word adds it, split into its int32 parts, to the
-// int64 buffer (rows i < n, columns j <= i; the block's other entries hold
-// nothing) and zeroes it.  Each int64 value has one writer.
-__global__ void fold_words_kernel(uint64_t *words, int64_t *state, int n, long long nbaseline,
-                                  long long nblk, long long total) {
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const long long blkg = idx >> 12;
-    const int w = (int)(idx & 4095);
-    const int f = (int)(blkg / nblk);
-    const long long k = blkg - (long long)f * nblk;
-    int rb = (int)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
-    while ((long long)rb * (rb + 1) / 2 > k) --rb;
-    while ((long long)(rb + 1) * (rb + 2) / 2 <= k) ++rb;
-    const int cb = (int)(k - (long long)rb * (rb + 1) / 2);
-    const int q = w >> 10, jl = (w >> 5) & 31, ilq = (w >> 2) & 7, pp = w & 3;
-    const long long i = (long long)rb * kStations + 8 * q + ilq;
-    const long long j = (long long)cb * kStations + jl;
-    const uint64_t word = words[idx];
-    if (word != 0 && i < n && j <= i) {
-      const long long re = (long long)(int)(uint32_t)word;                  // low part, signed
-      const long long im = (long long)(word - (unsigned long long)re) >> 32;  // exact: |re| < 2^31
-      int64_t *d = state + (((long long)f * nbaseline + i * (i + 1) / 2 + j) * 4 + pp) * 2;
-      d[0] += re;
-      d[1] += im;
-    }
-    if (word != 0) words[idx] = 0;
+// The fold: one CTA per quarter of a 32x32-station block of one channel
+// (grid x = 4 * block within the channel's triangle of blocks + quarter q,
+// y = channel): the quarter's 1024 words, rows 8q..8q+7 of the block, are 8 KB
+// contiguous, [column jl][row ilq][product pp].  The CTA reads them with
+// contiguous 16-byte loads into shared memory (columns padded to 36 words, so
+// that the reads below take the minimum two wavefronts); warp ilq then adds
+// its row's words, split into their int32 parts, to the row's 32 int64
+// (re, im) pairs of each product -- or stores them there (store_state: the
+// int64 buffer holds nothing yet) -- 2 KB contiguous, four 512-byte loads and
+// stores per warp, all loads first.  Rows i < n, columns j <= i only (the
+// block's other entries hold nothing).  Each int64 value has one writer.  The
+// words are left as they are: the next launch that uses them stores its own
+// (or they are cleared first).  Launched programmatically behind the engine
+// launch that filled the words: it waits for that launch (and so for the
+// chain before it) before touching memory, and lets the next launch start its
+// prologue at once.
+constexpr int kFoldColWords = 36;
+__global__ void __launch_bounds__(256) fold_words_kernel(const uint64_t *__restrict__ words,
+                                                         int64_t *__restrict__ state, int n,
+                                                         long long nbaseline, int nblk,
+                                                         int store_state) {
+  __shared__ __align__(16) unsigned long long sw[32 * kFoldColWords];
+  pdl_wait();
+  pdl_trigger();
+  const int k = blockIdx.x >> 2, f = blockIdx.y, q = blockIdx.x & 3;
+  int rb = (int)((sqrtf(8.0f * (float)k + 1.0f) - 1.0f) * 0.5f);
+  while (rb * (rb + 1) / 2 > k) --rb;
+  while ((rb + 1) * (rb + 2) / 2 <= k) ++rb;
+  const int cb = k - rb * (rb + 1) / 2;
+  const ulonglong2 *src =
+      reinterpret_cast<const ulonglong2 *>(words + ((long long)f * nblk + k) * 4096 + q * 1024);
+  const int t = threadIdx.x;
+  const ulonglong2 a0 = src[t], a1 = src[t + 256];   // words 2t, 2t+1 and 512 + 2t, 513 + 2t
+  const int ilq = t >> 5, lane = t & 31;
+  const long long i = (long long)rb * kStations + q * 8 + ilq;
+  const bool row_live = i < n;
+  const long long jbase = (long long)cb * kStations;
+  longlong2 *d = reinterpret_cast<longlong2 *>(
+      state + ((long long)f * nbaseline + (row_live ? i * (i + 1) / 2 : 0) + jbase) * 8);
+  // lane's products: column r * 8 + lane / 4, product lane % 4, r = 0..3
+  longlong2 acc[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    acc[r] = make_longlong2(0, 0);
+    if (!store_state && row_live && jbase + r * 8 + (lane >> 2) <= i) acc[r] = d[r * 32 + lane];
+  }
+  {
+    // word w = jl * 32 + ilq * 4 + pp goes to sw[jl * 36 + ilq * 4 + pp]
+    const int w0 = 2 * t, w1 = 512 + 2 * t;
+    *reinterpret_cast<ulonglong2 *>(&sw[(w0 >> 5) * kFoldColWords + (w0 & 31)]) = a0;
+    *reinterpret_cast<ulonglong2 *>(&sw[(w1 >> 5) * kFoldColWords + (w1 & 31)]) = a1;
+  }
+  __syncthreads();
+  if (!row_live) return;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int jl = r * 8 + (lane >> 2);
+    if (jbase + jl > i) continue;
+    const unsigned long long v = sw[jl * kFoldColWords + ilq * 4 + (lane & 3)];
+    const long long re = (long long)(int)(uint32_t)v;                   // low part, signed
+    const long long im = (long long)(v - (unsigned long long)re) >> 32;  // exact: |re| < 2^31
+    acc[r].x += re;
+    acc[r].y += im;
+    d[r * 32 + lane] = acc[r];
   }
 }
 
@@ -846,6 +891,13 @@ bool tc2_uses_words(int tcount, const TcTuning &tune) {
   return per <= tc2::kSplitEpilogueSteps;
 }
 
+bool tc2_single_item(int tcount, const TcTuning &tune) {
+  const int total_steps = (tcount + tc2::kKt - 1) / tc2::kKt;
+  int ksplit = tune.ksplit < 1 ? 1 : (tune.ksplit > total_steps ? total_steps : tune.ksplit);
+  const int per = (total_steps + ksplit - 1) / ksplit;
+  return (total_steps + per - 1) / per == 1;
+}
+
 long long words_blocks(const Sizes &s) {
   const long long nb = (s.n + tc2::kStations - 1) / tc2::kStations;
   return nb * (nb + 1) / 2;
@@ -853,13 +905,20 @@ long long words_blocks(const Sizes &s) {
 
 long long words_elems(const Sizes &s) { return (long long)s.f * words_blocks(s) * 4096; }
 
-cudaError_t launch_fold_words(uint64_t *words, int64_t *state, const Sizes &s, cudaStream_t st) {
-  const long long total = words_elems(s);
-  long long b = (total + 255) / 256;
-  if (b > 148LL * 16) b = 148LL * 16;
-  tc2::fold_words_kernel<<<(unsigned)b, 256, 0, st>>>(words, state, s.n, s.nbaseline,
-                                                       words_blocks(s), total);
-  return cudaGetLastError();
+cudaError_t launch_fold_words(const uint64_t *words, int64_t *state, const Sizes &s,
+                              cudaStream_t st, int overlap, int store_state) {
+  if (s.f > 65535) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(4 * words_blocks(s)), (unsigned)s.f);
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = overlap ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, tc2::fold_words_kernel, words, state, s.n, s.nbaseline,
+                            (int)words_blocks(s), store_state);
 }
 
 cudaError_t tc2_set_smem_attribute() {
@@ -872,7 +931,8 @@ cudaError_t tc2_set_smem_attribute() {
 
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune, int overlap,
-                       int f0, int fcount, const void *packed_in, uint64_t *words) {
+                       int f0, int fcount, const void *packed_in, uint64_t *words,
+                       int words_store) {
   if (fcount < 0) fcount = s.f - f0;
   if (f0 < 0 || fcount < 1 || f0 + fcount > s.f) return cudaErrorInvalidValue;
   const bool packed = packed_in != nullptr;   // `map` describes it (make_packed_map)
@@ -917,10 +977,13 @@ cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcoun
   p.total = j.items;
   p.err = err;
   p.stall = tune.stall;
-  p.overlap = (overlap && !overwrite) ? 1 : 0;
-  // word mode: adding launches of short items (tc2_uses_words), split epilogue
+  // word mode: launches of short items (tc2_uses_words), split epilogue; a
+  // launch that stores its words has one item per tile and overlaps nothing
   p.words = (!overwrite && per <= tc2::kSplitEpilogueSteps) ? words : nullptr;
   p.words_nblk = words_blocks(s);
+  p.words_store = (p.words && words_store) ? 1 : 0;
+  if (p.words_store && ksplit > 1) return cudaErrorInvalidValue;
+  p.overlap = (overlap && !overwrite && !p.words_store) ? 1 : 0;
   p.split_epi = (p.words || per <= tc2::kSplitEpilogueSteps) ? 1 : 0;
   int clusters = (tune.grid > 0 ? tune.grid : num_sms) / 2;
   if (clusters > p.total) clusters = p.total;
@@ -962,6 +1025,7 @@ cudaError_t launch_tc2_batch(const Job *dev_jobs, int njobs, int total_items, in
   p.overlap = 0;
   p.words = nullptr;
   p.words_nblk = 0;
+  p.words_store = 0;
   p.split_epi = max_item_steps <= tc2::kSplitEpilogueSteps ? 1 : 0;
   int clusters = (grid > 0 ? grid : sms) / 2;
   if (clusters > total_items) clusters = total_items;

@@ -95,29 +95,38 @@ cudaError_t launch_tc(const CUtensorMap &map, const Sizes &s, int t0, int tcount
 // packed_in != nullptr: the input is packed 4+4-bit, at packed_in with
 // geometry s (the pointer `map` was made from with make_packed_map), and the
 // CTA-pair kernel loads and expands it itself; it needs tune.wide.
-// words != nullptr (CTA-pair kernel, adding launches): the launch adds its
-// sums to the block-major word buffer `words` (words_elems(s) words) instead
-// of `state`; launch_fold_words later adds them into `state`.  At most 65535
-// samples may go into the words between folds.
+// words != nullptr (CTA-pair kernel, overwrite = 0): the launch puts its
+// sums into the block-major word buffer `words` (words_elems(s) words) instead
+// of `state` -- adding them, or storing them with words_store (only with one
+// item per tile, tc2_single_item) -- and launch_fold_words later moves them
+// into `state`.  At most 65535 samples may go into the words between folds.
 cudaError_t launch_tc_tuned(const CUtensorMap &map, const Sizes &s, int t0, int tcount,
                             int64_t *state, int overwrite, int *err, cudaStream_t st,
                             const TcTuning &tune, int overlap, int f0 = 0, int fcount = -1,
-                            const void *packed_in = nullptr, uint64_t *words = nullptr);
+                            const void *packed_in = nullptr, uint64_t *words = nullptr,
+                            int words_store = 0);
 // The CTA-pair (cta_group::2, 256x256 tile) kernel for one job.
 cudaError_t launch_tc2(const CUtensorMap &map, const Sizes &s, int t0, int tcount, int64_t *state,
                        int overwrite, int *err, cudaStream_t st, const TcTuning &tune,
                        int overlap, int f0 = 0, int fcount = -1,
-                       const void *packed_in = nullptr, uint64_t *words = nullptr);
+                       const void *packed_in = nullptr, uint64_t *words = nullptr,
+                       int words_store = 0);
 // Word buffer: 64-bit words (im * 2^32 + re of one visibility's sums) in
 // 32 x 32-station blocks; its size for sizes s, and the fold that adds the
-// words into the int64 buffer (triangular order) and zeroes them.  Exact while
-// every sum in the words is below 2^31 in magnitude (65535 samples).
+// words into the int64 buffer (triangular order).  Exact while every sum in
+// the words is below 2^31 in magnitude (65535 samples).
 long long words_blocks(const Sizes &s);   // 32-station blocks per channel
-// Whether an adding CTA-pair launch of tcount samples with `tune` adds words
-// (its items are short enough for the split epilogue).
+// Whether a CTA-pair launch of tcount samples with `tune` may use words (its
+// items are short enough for the split epilogue), and whether it has one item
+// per tile (no time splits: it may store its words).
 bool tc2_uses_words(int tcount, const TcTuning &tune);
+bool tc2_single_item(int tcount, const TcTuning &tune);
 long long words_elems(const Sizes &s);
-cudaError_t launch_fold_words(uint64_t *words, int64_t *state, const Sizes &s, cudaStream_t st);
+// overlap: the launch before it on `st` is an engine launch of the same
+// context (it may then start while that launch finishes).  store_state: the
+// int64 buffer holds nothing yet; the fold stores into it instead of adding.
+cudaError_t launch_fold_words(const uint64_t *words, int64_t *state, const Sizes &s,
+                              cudaStream_t st, int overlap = 0, int store_state = 0);
 constexpr int kWordsMaxSamples = 65535;
 // A batch of jobs from a device-resident table (item_begin ascending); with a
 // queue (device int) the CTAs take items dynamically, otherwise by stride.

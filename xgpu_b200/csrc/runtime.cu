@@ -86,14 +86,16 @@ struct Internal {
   // of device-resident input here (on s_conv) before converting them.
   void *d_slice = nullptr;
   void *d_state = nullptr;             // integration buffer
-  // Adding launches of the CTA-pair kernel add their sums to this word
-  // buffer (one 64-bit word per visibility, im * 2^32 + re: half the bytes of
-  // the int64 buffer's pairs); a fold adds the words into d_state before it
-  // is read and before more than kWordsMaxSamples samples have gone in.
-  // nullptr: no word buffer (it could not be allocated, or another engine).
+  // Launches of the CTA-pair kernel with short items put their sums into
+  // this word buffer (one 64-bit word per visibility, im * 2^32 + re: half
+  // the bytes of the int64 buffer's pairs); a fold moves the words into
+  // d_state before it is read and before more than kWordsMaxSamples samples
+  // have gone in.  nullptr: no word buffer (it could not be allocated, or
+  // another engine).
   uint64_t *d_words = nullptr;
   long long words_samples = 0;         // samples in the words since the last fold
-  bool words_dirty = false;
+  bool words_dirty = false;            // the words hold sums not yet in d_state
+  bool words_stale = false;            // the words hold nothing, but are not zero
   void *d_out = nullptr;               // formatted dump
   int *d_err = nullptr;                // device error word
   int *h_err = nullptr;                // pinned copy of it
@@ -273,22 +275,33 @@ bool packed_in_kernel(const Internal *in) {
 // input read in place, x then pointing at the context's first channel).
 // Add the words into the int64 buffer (and zero them), on s_comp after
 // everything queued there: before the buffer is read, and before the words
-// would hold more than kWordsMaxSamples samples.  An ordinary launch: the
-// next engine launch does not overlap it.
-int fold_words(Internal *in) {
+// would hold more than kWordsMaxSamples samples.  after_adding: the last
+// launch on s_comp is an adding engine launch of this context, which the fold
+// may then start beside (it waits for it before touching memory).  The next
+// engine launch does not overlap the fold; it only starts its prologue early.
+int fold_words(Internal *in, bool after_adding = false) {
   if (!in->words_dirty) return XGPU_OK;
-  XGPU_CHECK(launch_fold_words(in->d_words, (int64_t *)in->d_state, in->szc, in->s_comp));
+  // an integration held only in the words is stored into d_state
+  XGPU_CHECK(launch_fold_words(in->d_words, (int64_t *)in->d_state, in->szc, in->s_comp,
+                               after_adding && in->s_comp == in->s_own ? 1 : 0,
+                               in->state_zero ? 1 : 0));
+  in->state_zero = false;
   in->words_dirty = false;
+  in->words_stale = true;
   in->words_samples = 0;
   in->adding_tail = false;
   return XGPU_OK;
 }
 
 // *tail: in, the launch may overlap the adding launch before it; out, the
-// last launch queued only added.  allow_words: adding launches of the
-// CTA-pair kernel may add into the word buffer.
+// last launch queued only added.  allow_words: launches of the CTA-pair
+// kernel with short items may put their sums into the word buffer.  The first
+// launch into the int64 buffer while it holds nothing (state_zero) stores;
+// *wrote_state (if given) tells whether any launch went there, after which
+// the caller clears state_zero.
 int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fcount, bool *tail,
-                  bool packed = false, bool allow_words = true) {
+                  bool packed = false, bool allow_words = true, bool *wrote_state = nullptr) {
+  if (wrote_state) *wrote_state = true;
   const int ow = in->state_zero ? 1 : 0;
   if (!in->int_state) {
     XGPU_CHECK(launch_plain_fp32(x, s, 0, s.t, (float *)in->d_state, ow, in->s_comp, in->d_err,
@@ -308,26 +321,44 @@ int launch_engine(Internal *in, const int8_t *x, const Sizes &s, int f0, int fco
       fprintf(stderr, "xgpu: cannot describe the input buffer to the tensor memory accelerator\n");
       return XGPU_CUDA_ERROR;
     }
+    bool state_written = false;
     for (int t0 = 0; t0 < s.t; t0 += kSegment) {
       const int tc = s.t - t0 < kSegment ? s.t - t0 : kSegment;
-      const int store = ow && t0 == 0;
-      const bool words = allow_words && in->d_words && in->tune.wide && !store &&
-                         tc2_uses_words(tc, in->tune);
-      if (words && in->words_samples + tc > kWordsMaxSamples) {
-        const int r = fold_words(in);
+      const bool words = allow_words && in->d_words && in->tune.wide && tc2_uses_words(tc, in->tune);
+      if (!words) {
+        const int store = in->state_zero && !state_written ? 1 : 0;
+        XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
+                                   in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount,
+                                   packed ? (const void *)x : nullptr));
+        state_written = true;
+        *tail = !store;   // the next segment follows an adding launch
+        continue;
+      }
+      if (in->words_samples + tc > kWordsMaxSamples) {
+        const int r = fold_words(in, *tail);
         if (r != XGPU_OK) return r;
-        *tail = false;   // the fold is an ordinary launch
+        *tail = false;
       }
-      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, store, in->d_err,
-                                 in->s_comp, in->tune, *tail && !store ? 1 : 0, f0, fcount,
-                                 packed ? (const void *)x : nullptr,
-                                 words ? in->d_words : nullptr));
-      if (words) {
-        in->words_samples += tc;
-        in->words_dirty = true;
+      // Words that hold nothing are overwritten by a launch with one item per
+      // tile; a launch with time splits adds, into words cleared first.
+      int wstore = 0;
+      if (!in->words_dirty) {
+        if (tc2_single_item(tc, in->tune)) {
+          wstore = 1;
+        } else if (in->words_stale) {
+          XGPU_CHECK(cudaMemsetAsync(in->d_words, 0, (size_t)words_elems(in->szc) * 8, in->s_comp));
+          *tail = false;
+        }
       }
-      *tail = !store;   // the next segment follows an adding launch
+      XGPU_CHECK(launch_tc_tuned(*map, s, t0, tc, (int64_t *)in->d_state, 0, in->d_err, in->s_comp,
+                                 in->tune, *tail && !wstore ? 1 : 0, f0, fcount,
+                                 packed ? (const void *)x : nullptr, in->d_words, wstore));
+      in->words_samples += tc;
+      in->words_dirty = true;
+      in->words_stale = false;
+      *tail = !wstore;   // the next segment may overlap only a launch that added
     }
+    if (wrote_state) *wrote_state = state_written;
   }
   return XGPU_OK;
 }
@@ -388,10 +419,11 @@ int run_engine(Internal *in, const void *d_input, cudaEvent_t input_ready, bool 
       geom = &in->sz;
     }
   }
-  const int r = launch_engine(in, x, *geom, 0, s.f, &tail, packed);
+  bool wrote_state = true;
+  const int r = launch_engine(in, x, *geom, 0, s.f, &tail, packed, true, &wrote_state);
   if (r != XGPU_OK) return r;
   if (in->int_state) in->adding_tail = tail && conv < 0;   // tensor or dp4a engine
-  in->state_zero = false;
+  if (wrote_state) in->state_zero = false;   // otherwise the call went to the words
   if (conv >= 0) {
     XGPU_CHECK(cudaEventRecord(in->conv_free[conv], in->s_comp));
     in->conv_used[conv] = true;
@@ -434,12 +466,13 @@ void *direct_output(XGPUContext *ctx, Internal *in) {
 }
 
 int dump(XGPUContext *ctx, Internal *in) {
+  const bool after_adding = in->adding_tail;
   in->adding_tail = false;
   if (!in->matrix_h_set || !ctx->matrix_h) return XGPU_HOST_BUFFER_NOT_SET;
   if (ctx->matrix_len && ctx->output_offset + (size_t)in->sz.mat_length > ctx->matrix_len)
     return XGPU_INVALID_ARGUMENT;
   {
-    const int r = fold_words(in);
+    const int r = fold_words(in, after_adding);
     if (r != XGPU_OK) return r;
   }
   if (in->state_zero) {
@@ -811,11 +844,11 @@ int xgpuClearDeviceIntegrationBuffer(XGPUContext *context) {
   Internal *in = get(context);
   if (!in) return XGPU_NOT_INITIALIZED;
   XGPU_CHECK(cudaSetDevice(in->device));
-  // Ordered after queued engine launches; the next launch overwrites.  Words
-  // not yet folded belong to the integration being discarded.
+  // The next launch into either buffer overwrites it (or clears it first).
+  // Words not yet folded belong to the integration being discarded.
   if (in->words_dirty) {
-    XGPU_CHECK(cudaMemsetAsync(in->d_words, 0, (size_t)words_elems(in->szc) * 8, in->s_comp));
     in->words_dirty = false;
+    in->words_stale = true;
     in->words_samples = 0;
   }
   in->adding_tail = false;
@@ -986,10 +1019,11 @@ int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_o
   if (!in) return XGPU_NOT_INITIALIZED;
   if (!host_out || !in->int_state) return XGPU_INVALID_ARGUMENT;
   XGPU_CHECK(cudaSetDevice(in->device));
+  const bool after_adding = in->adding_tail;
   in->adding_tail = false;
   const size_t bytes = (size_t)in->sz.state_elems * 8;
   {
-    const int r = fold_words(in);
+    const int r = fold_words(in, after_adding);
     if (r != XGPU_OK) return r;
   }
   if (in->state_zero) {
@@ -1000,6 +1034,13 @@ int xgpuDumpDeviceIntegrationBufferInt64(XGPUContext *context, long long *host_o
   XGPU_CHECK(cudaMemcpyAsync(host_out, in->d_state, bytes, cudaMemcpyDeviceToHost, in->s_comp));
   XGPU_CHECK(cudaStreamSynchronize(in->s_comp));
   return check_device_error(in);
+}
+
+int xgpuFlushIntegrationBuffer(XGPUContext *context) {
+  Internal *in = get(context);
+  if (!in) return XGPU_NOT_INITIALIZED;
+  XGPU_CHECK(cudaSetDevice(in->device));
+  return fold_words(in, in->adding_tail);
 }
 
 int xgpuSetComputeStream(XGPUContext *context, void *stream) {
