@@ -4,10 +4,13 @@
                                      [--reps 5] [--warmup 3] [--ksplit K] [--pair P]
                                      [--grid G] [--accumulate] [--caller-stream]
                                      [--format int8|packed4|dp4a_swizzled|block32] [--dump]
+                                     [--flush]
 
 Prints one JSON line: milliseconds per xgpuCudaXengineDevice call (CUDA
 events on the engine's stream), X-engine TOPS (16*F*T*N(N+1) ops per call)
-and the host time to queue one call (when it approaches the device time, the
+(with --flush the timed region ends with xgpuFlushIntegrationBuffer, which
+adds the CTA-pair kernel's short-term per-call sums into the integration
+buffer) and the host time to queue one call (when it approaches the device time, the
 caller, not the GPU, sets the pace).  Useful to size a deployment and as a small, self-contained case for
 profilers.
 """
@@ -39,6 +42,8 @@ def main():
                     help="input format (converted on the device before the engine)")
     ap.add_argument("--dump", action="store_true",
                     help="dump (device formatting + copy to the host) after every call")
+    ap.add_argument("--flush", action="store_true",
+                    help="end the timed region with xgpuFlushIntegrationBuffer")
     args = ap.parse_args()
 
     import torch
@@ -73,6 +78,8 @@ def main():
             c.clear()
         c.run_device(x.data_ptr(), sync)
     host_ms = (time.perf_counter() - h0) * 1e3 / args.reps
+    if args.flush:
+        c.flush()
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.reps
@@ -80,7 +87,8 @@ def main():
     tuning = c.tuning() if engine == "tensor" else None
     print(json.dumps({"engine": c.engine_name, "n": args.n, "f": args.f, "t": args.t,
                       "ms": ms, "tops": ops / (ms * 1e-3) / 1e12, "host_enqueue_ms": host_ms,
-                      "accumulate": args.accumulate, "tuning": tuning}))
+                      "accumulate": args.accumulate, "flush": args.flush,
+                      "tuning": tuning}))
     c.close()
 
 
