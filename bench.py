@@ -762,9 +762,10 @@ def main():
                 "frac": hbm_ach / hbm_peak, "traffic": traffic,
                 "peak_source": f"hbm_gbs of {peak_src} (of measured)",
                 "algorithmic_bytes_per_launch": alg_bytes,
-                "note": "algorithmic bytes = input + int64 buffer read and written; the buffer "
-                        "stays in L2 between calls, so DRAM sees less (traffic: ncu, cold "
-                        "stand-alone launch)"}
+                "note": "algorithmic bytes = input + int64 buffer read and written; adding "
+                        "launches keep the call's sums in a word buffer of half those bytes, "
+                        "which stays in L2 between calls, so DRAM sees less (traffic: ncu, "
+                        "cold stand-alone launch: input + words)"}
     else:
         roof = {"bound": "tensor", "kernel": kernel, "achieved": tops_ach, "peak": peak8, "unit": "TOPS",
                 "frac": tops_ach / peak8, "traffic": traffic,
