@@ -154,9 +154,10 @@ WORD_MAX_SAMPLES = 65535
 
 def word_folds(tuning, t, warmup, steps):
     """Launches of the library's fold kernel inside a timed run of `steps`
-    calls after `warmup` (the first warm-up call stores): CTA-pair launches
-    whose items take at most 8 stages of 128 samples add into a word buffer,
-    folded before it would pass 65535 samples and once at the closing flush."""
+    calls after `warmup`: CTA-pair launches whose items take at most 8 stages
+    of 128 samples put their sums into a word buffer (the first call of the
+    integration stores its words, the others add), folded before it would
+    pass 65535 samples and once at the closing flush."""
     if not tuning or not tuning["pair"]:
         return 0
     stages = -(-t // 128)
@@ -164,7 +165,7 @@ def word_folds(tuning, t, warmup, steps):
     if -(-stages // ksplit) > 8:
         return 0
     samples, folds = 0, 0
-    for k in range(1, warmup + steps):
+    for k in range(warmup + steps):
         if samples + t > WORD_MAX_SAMPLES:
             folds += k >= warmup
             samples = 0

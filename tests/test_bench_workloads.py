@@ -68,3 +68,18 @@ def test_channel_input_is_the_channel_of_the_generated_block(oracle_mod):
                 want = oracle_mod.unpack4(want)
             got = bench.channel_input(oracle_mod, kind, 9000, 40.0, n, f_total, t, f)
             assert np.array_equal(got, want)
+
+
+def test_fold_launches_counted_in_the_timed_region():
+    """gpu_launches counts the word buffer's folds: the words take every call
+    from the first one, a fold comes before they would pass 65535 samples
+    (calls 63, 126, 189 at T=1024) and one closes the timed region."""
+    pair = {"pair": 1, "ksplit": 1}
+    assert bench.word_folds(pair, 1024, 5, 20) == 1
+    assert bench.word_folds(pair, 1024, 10, 200) == 4
+    assert bench.word_folds(pair, 1024, 70, 3) == 1      # the fold at call 63 is in warm-up
+    assert bench.word_folds(pair, 1024, 63, 3) == 2      # call 63 is timed
+    assert bench.word_folds(pair, 8192, 3, 20) == 0      # 64-stage items: int64 buffer
+    assert bench.word_folds({"pair": 1, "ksplit": 8}, 8192, 3, 20) == 4   # calls 7, 14, 21 + 1
+    assert bench.word_folds({"pair": 0, "ksplit": 1}, 1024, 3, 20) == 0
+    assert bench.word_folds(None, 1024, 3, 20) == 0
