@@ -321,13 +321,13 @@ void *xgpuComputeStream(XGPUContext *context);
  * XGPU_INVALID_ARGUMENT, as do the sizes xgpuInitEx rejects and a channel
  * range (channel_offset / input_nfrequency other than the whole input).  Work
  * is queued on `stream` (a cudaStream_t, NULL for the legacy default stream)
- * and the call waits for it and reads its error status back to the host, so
- * it is synchronous and cannot be recorded into a CUDA graph.  The calling
- * thread's current device is left as it was.  All calls share the array:
- * calls that overlap on the GPU race and must be serialised.  The first call
- * on a device looks up the array's device address and keeps it for the
- * process's lifetime; after a cudaDeviceReset of that device the address is
- * stale, so make no further call on it. */
+ * and the call waits for it and reads its error status back to the host
+ * before it returns.  The calling thread's current device is left as it was.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialised.  The first call on a device looks up the array's device address
+ * and keeps it for the process's lifetime, so make that first call before any
+ * stream capture begins; after a cudaDeviceReset of that device the address
+ * is stale, so make no further call on it. */
 int xgpuCorrelateStatic(const void *device_input, void *device_output, const XGPUConfig *cfg,
                         int device, void *stream);
 

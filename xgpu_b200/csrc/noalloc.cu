@@ -27,10 +27,12 @@
 // once per device with that device current, on the first call made on that
 // device, and kept for the life of the process (a cudaDeviceReset of that
 // device invalidates it: make no call on a device after resetting it).
+// Because that first call does this set-up, make it before any stream
+// capture begins.
 //
 // Every call waits for its own work (cudaStreamSynchronize) and reads the
-// error word back into host memory, so a call cannot be recorded into a CUDA
-// graph.  The caller's current device is the same after the call as before.
+// error word back into host memory.  The caller's current device is the same
+// after the call as before.
 #include <string.h>
 
 #include <mutex>
