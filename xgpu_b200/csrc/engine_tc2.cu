@@ -14,9 +14,9 @@
 //   * per CTA and per 128 samples that is 32 KiB of loads for 128x256 output
 //     columns -- half the bytes per MMA operation of the single-CTA kernel, so
 //     the load pipeline's latency is covered with the same shared memory.
-// Cross-CTA signalling uses no multicast: TMA loads of both CTAs complete on
-// the leader's "full" barrier (.cta_group::2 form, the peer's copy names the
-// leader's barrier; only the leader registers the expected bytes, so the
+// Cross-CTA signalling: each CTA's TMA loads fill only its own shared memory
+// and complete on the leader's "full" barrier (.cta_group::2 form, the peer's
+// copy names the leader's barrier; only the leader registers the expected bytes, so the
 // producers issue no cross-CTA fence), the leader's MMA commits once to each CTA's "empty" and
 // "accumulator full" barriers, and the peer's epilogue arrives remotely on the
 // leader's "accumulator empty" barrier.  Every wait is bounded (as in
