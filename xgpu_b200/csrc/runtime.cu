@@ -118,14 +118,18 @@ struct Internal {
   // next accumulating launch over other input may overlap it.
   bool adding_tail = false;
 
-  // tensor maps, cached by device pointer
+  // tensor maps, cached by device pointer: enough entries for a pipeline
+  // that rotates over a ring of input buffers (a miss costs a host-side
+  // encode per call); replaced round-robin
+  static constexpr int kMaps = 16;
   struct MapEntry {
     const void *ptr;
     bool packed;     // packed 4+4-bit geometry (make_packed_map)
     int fin;         // channels per sample of the buffer
     CUtensorMap map;
-  } maps[4];
+  } maps[kMaps];
   int nmaps = 0;
+  int next_map = 0;   // the entry a miss replaces once all are in use
 
   ComplexInput *free_array_h = nullptr, *unregister_array_h = nullptr;
   bool array_h_set = false, register_host_array = true;
@@ -247,7 +251,13 @@ const CUtensorMap *tensor_map(Internal *in, const void *ptr, const Sizes &g, boo
   for (int q = 0; q < in->nmaps; ++q)
     if (in->maps[q].ptr == ptr && in->maps[q].packed == packed && in->maps[q].fin == g.fin)
       return &in->maps[q].map;
-  const int slot = in->nmaps < 4 ? in->nmaps++ : 3;
+  int slot;
+  if (in->nmaps < Internal::kMaps) {
+    slot = in->nmaps++;
+  } else {
+    slot = in->next_map;
+    in->next_map = (in->next_map + 1) % Internal::kMaps;
+  }
   const int r = packed ? make_packed_map(&in->maps[slot].map, ptr, g)
                        : make_tc_tensor_map(&in->maps[slot].map, ptr, g);
   if (r != 0) {
